@@ -1,0 +1,362 @@
+"""Benchmark: ms per Lucas-Lehmer iteration at the 3200K FFT (p = 57885161).
+
+One step = S LL iterations (default 10000, the reference's report interval)
+of one exponent, through the engine's C ABI.  With --gpus N (one process per
+GPU under torch.distributed.run) every rank runs its own independent test
+(replicas: LL iterations do not shard), the time is the max over ranks and
+`value` is that time divided by the iterations of all ranks.
+
+--impl reference runs the reference itself, CUDALucas v2.06 built from its
+sources for sm_100a (oracle/_ref/CUDALucas, cuFFT), on the same GPU and the
+same exponent and FFT length, and reports its own printed ms/iter.
+"""
+import argparse
+import json
+import os
+import re
+import signal
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (exponent, FFT length in words, description)
+    "3200K": (57885161, 3276800, "p=57885161 at 3200K (3276800 FP64 words, 17.665 bits/word)"),
+    "12K": (216091, 12288, "p=216091 at 12K (12288 FP64 words, 17.586 bits/word)"),
+    "18432K": (332192831, 18874368, "p=332192831 at 18432K (18874368 FP64 words, 17.600 bits/word)"),
+}
+METRIC = "ms/LL iter at 3.2M FFT vs ref cuFFT"
+
+
+def peaks():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(workload):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        return d.get(workload)
+    except Exception:
+        return None
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(q, n, iters):
+    """The oracle (plain C IBDWT restatement, one host core) on a bounded
+    sample of the same workload."""
+    from oracle.binding import Oracle
+    o = Oracle(q, n)
+    o.start(0)
+    o.step(1)
+    t = time.perf_counter()
+    o.step(iters)
+    dt = time.perf_counter() - t
+    return {"value": dt * 1000.0 / iters, "unit": "ms/iter", "cores": 1, "kind": "port",
+            "sample": "%d iterations of p=%d at n=%d (oracle/ibdwt_oracle.c, mixed-radix C FFT, 1 thread)"
+                      % (iters, q, n)}
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    import cudalucas_b200 as cl
+
+    q, n, desc = WORKLOADS[args.workload]
+    S, K, W = args.iters_per_step, args.steps, args.warmup
+    torch.cuda.set_device(local)
+    ctx = cl.LLContext(q, n, device=local)
+    ctx.start((rank * 7919) % q)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    for _ in range(W):
+        ctx.step(S)
+    ctx.sync()
+
+    # -- device-timed region: K steps of S iterations, L2 flushed between steps
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        for i in range(K):
+            with torch.cuda.stream(ext):
+                flush.zero_()
+                evs[i][0].record(ext)
+            ctx.step(S)
+            evs[i][1].record(ext)
+        ctx.sync()
+        torch.cuda.synchronize()
+    barrier(world)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = allreduce_max(sum(step_ms), world)
+    maxerr = ctx.step(1, report=True)
+
+    # -- per-pass timing on real iterations (roofline of the dominant kernel)
+    R = 200
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(R)]
+    for i in range(R):
+        ev[i][0].record(ext)
+        ctx.debug_launch(0)
+        ev[i][1].record(ext)
+        ctx.debug_launch(1)
+        ev[i][2].record(ext)
+    ctx.sync()
+    torch.cuda.synchronize()
+    t_tall = sum(e[0].elapsed_time(e[1]) for e in ev) / R
+    t_wide = sum(e[1].elapsed_time(e[2]) for e in ev) / R
+
+    # -- end to end through the public API with host buffers (pinned):
+    # load digits (H2D), S iterations, read digits (D2H), Res64 on the host
+    ctx.step(1, report=True)
+    d0, off0 = ctx.read_digits()
+    pinned_in = torch.from_numpy(d0).pin_memory()
+    pinned_out = torch.empty(n, dtype=torch.int32).pin_memory()
+    import ctypes
+    from cudalucas_b200 import native
+    L = native.lib()
+    pin_in = ctypes.cast(pinned_in.data_ptr(), ctypes.POINTER(ctypes.c_int32))
+    pin_out = ctypes.cast(pinned_out.data_ptr(), ctypes.POINTER(ctypes.c_int32))
+    offv = ctypes.c_uint32()
+    errv = ctypes.c_float()
+    E = max(1, min(K, 3))
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(E):
+        assert L.ll_load_digits(ctx._h, pin_in, off0) == 0
+        assert L.ll_step(ctx._h, S, 1, ctypes.byref(errv)) == 0
+        assert L.ll_read_digits(ctx._h, pin_out, ctypes.byref(offv)) == 0
+        res = L.ll_digits_res64(pin_out, q, n, offv.value)
+    e2e_ms = (time.perf_counter() - t0) * 1000.0
+    e2e_ms = allreduce_max(e2e_ms, world)
+    shape = ctx.shape
+    ctx.close()
+
+    if rank != 0:
+        return None
+    hbm, peak_kind = peaks()
+    dom, t_dom = ("wide", t_wide) if t_wide >= t_tall else ("tall", t_tall)
+    alg_bytes = 16.0 * n  # one read + one write of n FP64 words per pass
+    achieved = alg_bytes / (t_dom * 1e-3) / 1e9
+    traffic = ncu_traffic(args.workload)
+    out = {
+        "metric": METRIC,
+        "value": round(total_ms / (K * S * world), 6),
+        "unit": "ms/iter",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": round(total_ms / K, 4),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: LL test from s0=4 (no dataset)",
+        "config": {"workload": desc, "exponent": q, "fft_words": n, "iters_per_step": S,
+                   "per_gpu_ms_per_iter": round(total_ms / (K * S), 6),
+                   "shape": shape, "max_roundoff_error": round(maxerr, 6),
+                   "bits_per_word": round(q / n, 4),
+                   "l2": "flushed (256 MB write) before each timed step; the 26 MB state stays "
+                         "L2-resident inside a step, as it does for the reference",
+                   "parallelism": "replicas (one independent exponent per GPU)"},
+        "e2e": {"value": round(e2e_ms / (E * S * world), 6) * world, "unit": "ms/iter",
+                "h2d_bytes_per_step": 4 * n + 32, "d2h_bytes_per_step": 4 * n + 32,
+                "steps": E, "path": "ll_load_digits -> ll_step(LL_REPORT) -> ll_read_digits -> ll_digits_res64"},
+        "roofline": {"bound": "hbm", "kernel": dom + "_kernel", "achieved": round(achieved, 1),
+                     "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                     "launch_us": {"tall": round(t_tall * 1000, 2), "wide": round(t_wide * 1000, 2)}},
+        "clocks": clk.summary(),
+        "gpu_launches": 2 * K * S,
+    }
+    if args.cpu_iters > 0:
+        out["cpu_baseline"] = cpu_baseline(q, n, args.cpu_iters)
+    return out
+
+
+def run_reference(args, world, rank, local):
+    """CUDALucas itself (oracle/_ref/CUDALucas) on this GPU: same exponent,
+    forced FFT length, report every S iterations; its printed wall-clock
+    ms/iter over W warm-up and K timed report intervals."""
+    if rank != 0:
+        return None
+    q, n, desc = WORKLOADS[args.workload]
+    S, K, W = args.iters_per_step, args.steps, args.warmup
+    exe = os.path.join(ROOT, "oracle", "_ref", "CUDALucas")
+    base = {"impl": "reference", "metric": METRIC, "unit": "ms/iter", "n_gpus": world, "steps": K,
+            "warmup": W, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic: LL test from s0=4 (no dataset)"}
+    if not os.path.exists(exe):
+        base["unavailable"] = "reference binary oracle/_ref/CUDALucas not built (make -C oracle ref)"
+        return base
+    work = tempfile.mkdtemp(prefix="cudalucas_ref_")
+    with open(os.path.join(work, "CUDALucas.ini"), "w") as f:
+        f.write("WorkFile=worktodo.txt\nResultsFile=results.txt\nSaveAllCheckpoints=0\n"
+                "SaveFolder=savefiles\nDeviceNumber=%d\nPrintDeviceInfo=0\nErrorIterations=100\n"
+                "ReportIterations=%d\nCheckpointIterations=%d\nPolite=0\nPoliteValue=50\nBigCarry=0\n"
+                "ErrorReset=85\nInteractive=0\nRoundoffTest=0\nThreads=256 128\nOutputHInterval=0\n"
+                "Sleep=0\nSleepValue=0\nErrorLimit=40\n" % (local, S, 100 * S * (W + K + 2)))
+    cmd = [exe, "-d", str(local), "-f", "%dK" % (n // 1024), "-x", str(S), str(q)]
+    rx = re.compile(r"Iteration (\d+) .*?0x([0-9a-f]{16}).*?error = ([0-9.]+).*?([0-9.]+) ms/iter")
+    rows = []
+    t0 = time.perf_counter()
+    p = subprocess.Popen(cmd, cwd=work, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,
+                         start_new_session=True)
+    log = []
+    try:
+        for line in p.stdout:
+            log.append(line.rstrip())
+            m = rx.search(line)
+            if m:
+                rows.append((int(m.group(1)), m.group(2), float(m.group(3)), float(m.group(4))))
+                if len(rows) >= W + K:
+                    break
+            if time.perf_counter() - t0 > 900:
+                break
+    finally:
+        try:
+            os.killpg(p.pid, signal.SIGINT)
+            p.wait(timeout=60)
+        except Exception:
+            os.killpg(p.pid, signal.SIGKILL)
+    if len(rows) < W + K:
+        base["unavailable"] = "reference produced %d report lines; tail: %s" % (len(rows), " | ".join(log[-3:]))
+        return base
+    timed = rows[W:W + K]
+    ms = statistics.mean(r[3] for r in timed)
+    base.update({
+        "value": round(ms, 6),
+        "ms_per_step": round(ms * S, 4),
+        "config": {"workload": desc, "exponent": q, "fft_words": n, "iters_per_step": S,
+                   "command": " ".join(cmd[1:]), "res64": {str(r[0]): r[1] for r in rows},
+                   "max_roundoff_error": max(r[2] for r in timed),
+                   "timing": "CUDALucas's own wall-clock ms/iter per report interval (includes its "
+                             "blocking error read-back every 100 iterations, CUDALucas.cu:2936)"},
+        "e2e": {"value": round(ms, 6), "unit": "ms/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": round(ms, 6), "unit": "ms/iter", "cores": 1, "kind": "reference",
+                         "sample": "%d report intervals of %d iterations of the reference binary "
+                                   "(GPU %d, driven by one host thread)" % (K, S, local)},
+    })
+    return base
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="3200K", choices=sorted(WORKLOADS))
+    ap.add_argument("--iters-per-step", type=int, default=10000)
+    ap.add_argument("--cpu-iters", type=int, default=20, help="oracle iterations for cpu_baseline (0: skip)")
+    args = ap.parse_args()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        out = run_reference(args, world, rank, local)
+    else:
+        out = run_ours(args, world, rank, local)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,819 @@
+// B200 Lucas-Lehmer engine: two fused FP64 passes per iteration.
+//
+// Replaces one call of CUDALucas's lucas_square (CUDALucas.cu:1869-1986):
+// cuFFT Z2Z -> square -> cuFFT Z2Z -> rcb -> splice, five launches that each
+// sweep the n-word array, become two kernels that each read and write it once.
+//
+// Data layout (N = n/2 complex elements, N = W * H):
+//   element m = m1*H + m2 holds words 2m (real) and 2m+1 (imaginary);
+//   the array at rest is A[k1][m2] (k1 < W, m2 < H) at address k1*H + m2,
+//   i.e. every column of the 2-D decomposition is contiguous in HBM.
+//
+// tall pass (one CTA per column pair k1, W-k1): twiddle w_N^(k1*m2), H-point
+//   FFT, real-signal pairing of bins k and N-k with pointwise squaring (the
+//   work of `square`, CUDALucas.cu:255-314), inverse H-point FFT, conjugate
+//   twiddle.
+// wide pass (one CTA per G consecutive rows m2): inverse W-point FFT,
+//   unweight, round, roundoff max, -2, carry, reweight (the work of rcb and
+//   splice, CUDALucas.cu:322-534), forward W-point FFT.
+//
+// Carries.  Word i keeps bal(low_i + c1_{i-1}) + c2_{i-1}, where c1 is the
+// high part of word i-1's rounded value and c2 the carry out of balancing
+// word i-1: the two-step carry that rcb applies inside its 128-word rows
+// (CUDALucas.cu:389-405).  Element m's outgoing pair (c1, c2) depends only on
+// element m's own two words, so the carry from the last row of CTA g to the
+// first row of CTA g+1 (and from the top word to word 0, the 2^q == 1 wrap of
+// carry_out[(blk+1) mod grid], CUDALucas.cu:474-483) is published once and
+// read once: a single bounded wait per CTA, no serial chain.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/llb200.h"
+#include "fft_device.cuh"
+
+namespace llb {
+
+constexpr int EPT = 16;  // max elements per thread in one FFT stage
+
+struct DevState {
+  unsigned long long ticket;  // wide-pass CTA ticket counter (monotonic)
+  uint32_t offset;            // shift of the current state (doubled by tall pass)
+  uint32_t err_bits;          // max roundoff error (float bits), reset by host
+  uint32_t fault;             // bit 0: wait timeout, bit 1: carry overflow
+  uint32_t pad_[3];
+};
+
+struct TallArgs {
+  double2 *A;
+  const double2 *twH;   // e^{2 pi i e/H}
+  const double2 *thi;   // e^{2 pi i (e<<TS)/N}
+  const double2 *tlo;   // e^{2 pi i e/N}, e < 2^TS
+  DevState *st;
+  FftPlan ph;
+  int W, H, N, ts, tmask;
+  uint32_t q;
+};
+
+struct WideArgs {
+  double2 *A;
+  int32_t *xint;
+  long long *carry;     // packed carries, one row of W per CTA
+  uint32_t *flags;      // one ready flag per CTA
+  const double2 *twW;
+  const int32_t *rowE;  // ((-(2*m2+t)*b) mod n), 2H entries
+  const double *rowW;   // 2^(rowE/n)
+  const double *rowWi;  // 2^(-rowE/n) / N
+  const int32_t *colF;  // ((-2*H*m1*b) mod n), W entries
+  const double *colW;
+  const double *colWi;
+  DevState *st;
+  FftPlan pw;
+  int W, H, G, ngroups;
+  uint32_t q, n, b, qn;
+};
+
+__device__ __forceinline__ double2 omegaN(const double2 *__restrict__ thi, const double2 *__restrict__ tlo,
+                                          int ts, int tmask, int e) {
+  return cmul(__ldg(&thi[e >> ts]), __ldg(&tlo[e & tmask]));
+}
+
+// Real-signal pairing and squaring of bins k and N-k (w = w_N^k):
+// E = (Z_k + conj Z_{N-k})/2, O = (Z_k - conj Z_{N-k})/(2i),
+// Z'_k = E^2 + w O^2 + 2iEO, Z'_{N-k} = conj(E^2 + w O^2 - 2iEO).
+__device__ __forceinline__ void pair_square(double2 &za, double2 &zb, double2 w) {
+  double2 E = make_double2(0.5 * (za.x + zb.x), 0.5 * (za.y - zb.y));
+  double2 O = make_double2(0.5 * (za.y + zb.y), -0.5 * (za.x - zb.x));
+  double2 E2 = make_double2((E.x - E.y) * (E.x + E.y), 2.0 * E.x * E.y);
+  double2 O2 = make_double2((O.x - O.y) * (O.x + O.y), 2.0 * O.x * O.y);
+  double2 P = cadd(E2, cmul(w, O2));
+  double2 EO = cmul(E, O);
+  double2 Q = make_double2(-2.0 * EO.y, 2.0 * EO.x);
+  za = cadd(P, Q);
+  zb = conjg(csub(P, Q));
+}
+
+template <int EPT_>
+__global__ void __launch_bounds__(256) tall_kernel(TallArgs a) {
+  extern __shared__ double2 sm[];
+  const int c = blockIdx.x;
+  const int W = a.W, H = a.H;
+  const bool special = (c == 0);
+  const int kA = special ? 0 : c;
+  const int kB = special ? W / 2 : W - c;
+  if (c == 0 && threadIdx.x == 0) {
+    // CUDALucas.cu:1882: offset <- 2*offset mod q, once per iteration
+    const uint32_t o = a.st->offset;
+    a.st->offset = (uint32_t)((2ull * o) % a.q);
+  }
+  for (int idx = threadIdx.x; idx < 2 * H; idx += blockDim.x) {
+    const int col = idx >= H;
+    const int m2 = idx - col * H;
+    const int k1 = col ? kB : kA;
+    double2 x = a.A[(size_t)k1 * H + m2];
+    double2 w = omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2);
+    sm[pad(idx)] = cmul(x, w);
+  }
+  __syncthreads();
+  if (2 * H <= EPT_ * (int)blockDim.x) {
+    fft_rows_b<EPT_, +1>(sm, a.ph, 2, 0, a.twH);
+  } else {
+    fft_rows_b<EPT_, +1>(sm, a.ph, 1, 0, a.twH);
+    fft_rows_b<EPT_, +1>(sm, a.ph, 1, 1, a.twH);
+  }
+  if (!special) {
+    for (int k2 = threadIdx.x; k2 < H; k2 += blockDim.x) {
+      double2 za = sm[pad(k2)], zb = sm[pad(2 * H - 1 - k2)];
+      pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, kA + W * k2));
+      sm[pad(k2)] = za;
+      sm[pad(2 * H - 1 - k2)] = zb;
+    }
+  } else {
+    const int half = H / 2;
+    for (int i = threadIdx.x; i <= half; i += blockDim.x) {  // column 0: k2 <-> (H-k2) mod H
+      const int p = (H - i) % H;
+      double2 za = sm[pad(i)], zb = sm[pad(p)];
+      pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W * i));
+      sm[pad(i)] = za;
+      if (p != i) sm[pad(p)] = zb;
+    }
+    for (int i = threadIdx.x; i < half; i += blockDim.x) {  // column W/2: k2 <-> H-1-k2
+      double2 za = sm[pad(H + i)], zb = sm[pad(2 * H - 1 - i)];
+      pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W / 2 + W * i));
+      sm[pad(H + i)] = za;
+      sm[pad(2 * H - 1 - i)] = zb;
+    }
+  }
+  __syncthreads();
+  if (2 * H <= EPT_ * (int)blockDim.x) {
+    fft_rows_b<EPT_, -1>(sm, a.ph, 2, 0, a.twH);
+  } else {
+    fft_rows_b<EPT_, -1>(sm, a.ph, 1, 0, a.twH);
+    fft_rows_b<EPT_, -1>(sm, a.ph, 1, 1, a.twH);
+  }
+  for (int idx = threadIdx.x; idx < 2 * H; idx += blockDim.x) {
+    const int col = idx >= H;
+    const int m2 = idx - col * H;
+    const int k1 = col ? kB : kA;
+    double2 w = omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2);
+    a.A[(size_t)k1 * H + m2] = cmulc(sm[pad(idx)], w);
+  }
+}
+
+struct WordInfo {
+  double w, wi;
+  int bits;
+};
+
+__device__ __forceinline__ WordInfo word_info(const WideArgs &a, int jr, int f, double cw, double cwi) {
+  WordInfo r;
+  const int e = __ldg(&a.rowE[jr]) + f;
+  const bool wrap = e >= (int)a.n;
+  const int ee = wrap ? e - (int)a.n : e;
+  r.w = __ldg(&a.rowW[jr]) * cw * (wrap ? 0.5 : 1.0);
+  r.wi = __ldg(&a.rowWi[jr]) * cwi * (wrap ? 2.0 : 1.0);
+  r.bits = (int)a.qn + (ee < (int)a.b ? 1 : 0);
+  return r;
+}
+
+// Outgoing carry of an element: (c1, c2) packed as c1 * 2^24 + c2.
+__device__ __forceinline__ long long pack_carry(long long c1, long long c2) { return (c1 << 24) + c2; }
+__device__ __forceinline__ void unpack_carry(long long p, long long &c1, long long &c2) {
+  c2 = (p << 40) >> 40;
+  c1 = (p - c2) >> 24;
+}
+
+__device__ __forceinline__ long long element_carry(long long v0, long long v1, int b0, int b1, uint32_t &fault) {
+  const long long h0 = v0 >> b0;
+  const long long low1 = v1 & ((1ll << b1) - 1);
+  const long long h1 = v1 >> b1;
+  const long long t1 = low1 + h0;
+  const long long k1 = (t1 + (1ll << (b1 - 1))) >> b1;
+  if (k1 >= (1ll << 23) || k1 < -(1ll << 23) || h1 >= (1ll << 38) || h1 < -(1ll << 38)) fault |= 2u;
+  return pack_carry(h1, k1);
+}
+
+__device__ __forceinline__ bool wait_flag(uint32_t *flag) {
+  for (int it = 0; it < (1 << 24); ++it) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+    if (v) return true;
+    __nanosleep(it < 64 ? 32 : 256);
+  }
+  return false;
+}
+
+enum { WIDE_ITER = 0, WIDE_REPORT = 1, WIDE_INIT = 2 };
+
+template <int EPT_, int MODE>
+__global__ void __launch_bounds__(256) wide_kernel(WideArgs a) {
+  extern __shared__ double2 sm[];
+  __shared__ int s_g;
+  __shared__ float s_err[32];
+  __shared__ uint32_t s_fault;
+  if (threadIdx.x == 0) {
+    s_fault = 0;
+    s_g = MODE == WIDE_INIT ? (int)blockIdx.x : (int)(atomicAdd(&a.st->ticket, 1ull) % (unsigned long long)a.ngroups);
+  }
+  __syncthreads();
+  const int g = s_g;
+  const int W = a.W, H = a.H, G = a.G;
+  const int m2b = g * G;
+  longlong2 *smi = reinterpret_cast<longlong2 *>(sm);
+  float emax = 0.f;
+  uint32_t fault = 0;
+
+  if (MODE != WIDE_INIT) {
+    for (int idx = threadIdx.x; idx < G * W; idx += blockDim.x) {
+      const int k1 = idx / G, r = idx - k1 * G;
+      sm[pad(r * W + k1)] = a.A[(size_t)k1 * H + m2b + r];
+    }
+    __syncthreads();
+    fft_rows_b<EPT_, -1>(sm, a.pw, G, 0, a.twW);
+
+    // -2 at bit (offset+1) mod q (CUDALucas.cu:1882-1886), exact integer math
+    const uint32_t off = a.st->offset;
+    const uint32_t pos = (off + 1) % a.q;
+    const uint32_t dw = (uint32_t)(((unsigned long long)pos * a.n) / a.q);
+    const uint32_t sdw = (uint32_t)(((unsigned long long)dw * a.q + a.n - 1) / a.n);
+    const long long sub = 1ll << (pos - sdw);
+
+    // phase A: unweight, round, error, -2; keep rounded words in place
+    for (int m1 = threadIdx.x; m1 < W; m1 += blockDim.x) {
+      const int f = __ldg(&a.colF[m1]);
+      const double cw = __ldg(&a.colW[m1]), cwi = __ldg(&a.colWi[m1]);
+      for (int r = 0; r < G; ++r) {
+        const int m2 = m2b + r;
+        const WordInfo w0 = word_info(a, 2 * m2, f, cw, cwi);
+        const WordInfo w1 = word_info(a, 2 * m2 + 1, f, cw, cwi);
+        const double2 u = sm[pad(r * W + m1)];
+        const double t0 = u.x * w0.wi, t1 = u.y * w1.wi;
+        const double r0 = rint(t0), r1 = rint(t1);
+        emax = fmaxf(emax, fabsf((float)(t0 - r0)));
+        emax = fmaxf(emax, fabsf((float)(t1 - r1)));
+        long long v0 = (long long)r0, v1 = (long long)r1;
+        const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
+        if (j0 == dw) v0 -= sub;
+        if (j0 + 1 == dw) v1 -= sub;
+        smi[pad(r * W + m1)] = make_longlong2(v0, v1);
+        if (r == G - 1) a.carry[(size_t)g * W + m1] = element_carry(v0, v1, w0.bits, w1.bits, fault);
+      }
+    }
+    __threadfence();
+    __syncthreads();
+    const int pred = g == 0 ? a.ngroups - 1 : g - 1;
+    if (threadIdx.x == 0) {
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&a.flags[g]), "r"(1u) : "memory");
+      if (!wait_flag(&a.flags[pred])) s_fault |= 1u;
+      a.flags[pred] = 0;
+    }
+    __syncthreads();
+
+    // phase B: carry in, balance, reweight (rows of this CTA in order)
+    for (int m1 = threadIdx.x; m1 < W; m1 += blockDim.x) {
+      const int f = __ldg(&a.colF[m1]);
+      const double cw = __ldg(&a.colW[m1]), cwi = __ldg(&a.colWi[m1]);
+      const int pm1 = g == 0 ? (m1 == 0 ? W - 1 : m1 - 1) : m1;
+      long long cin = __ldcg(&a.carry[(size_t)pred * W + pm1]);
+      for (int r = 0; r < G; ++r) {
+        const int m2 = m2b + r;
+        const WordInfo w0 = word_info(a, 2 * m2, f, cw, cwi);
+        const WordInfo w1 = word_info(a, 2 * m2 + 1, f, cw, cwi);
+        const longlong2 v = smi[pad(r * W + m1)];
+        long long C1, C2;
+        unpack_carry(cin, C1, C2);
+        const int b0 = w0.bits, b1 = w1.bits;
+        const long long low0 = v.x & ((1ll << b0) - 1), h0 = v.x >> b0;
+        const long long low1 = v.y & ((1ll << b1) - 1);
+        const long long t1 = low1 + h0;
+        const long long k1c = (t1 + (1ll << (b1 - 1))) >> b1;
+        const long long d1p = t1 - (k1c << b1);
+        const long long t0 = low0 + C1;
+        const long long k0 = (t0 + (1ll << (b0 - 1))) >> b0;
+        const long long d0p = t0 - (k0 << b0);
+        const long long d0 = d0p + C2, d1 = d1p + k0;
+        cin = element_carry(v.x, v.y, b0, b1, fault);
+        if (MODE == WIDE_REPORT) {
+          const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
+          a.xint[j0] = (int32_t)d0;
+          a.xint[j0 + 1] = (int32_t)d1;
+        }
+        sm[pad(r * W + m1)] = make_double2((double)d0 * w0.w, (double)d1 * w1.w);
+      }
+    }
+  } else {
+    // start / resume: weighted digits (apply_weights, CUDALucas.cu:216-249)
+    for (int m1 = threadIdx.x; m1 < W; m1 += blockDim.x) {
+      const int f = __ldg(&a.colF[m1]);
+      const double cw = __ldg(&a.colW[m1]), cwi = __ldg(&a.colWi[m1]);
+      for (int r = 0; r < G; ++r) {
+        const int m2 = m2b + r;
+        const WordInfo w0 = word_info(a, 2 * m2, f, cw, cwi);
+        const WordInfo w1 = word_info(a, 2 * m2 + 1, f, cw, cwi);
+        const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
+        sm[pad(r * W + m1)] = make_double2((double)a.xint[j0] * w0.w, (double)a.xint[j0 + 1] * w1.w);
+      }
+    }
+  }
+  __syncthreads();
+  fft_rows_b<EPT_, +1>(sm, a.pw, G, 0, a.twW);
+  for (int idx = threadIdx.x; idx < G * W; idx += blockDim.x) {
+    const int k1 = idx / G, r = idx - k1 * G;
+    a.A[(size_t)k1 * H + m2b + r] = sm[pad(r * W + k1)];
+  }
+  if (MODE != WIDE_INIT) {
+    // block max of the roundoff error -> atomicMax on the float bits
+#pragma unroll
+    for (int o = 16; o; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+    if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = emax;
+    if (fault) atomicOr(&s_fault, fault);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float m = 0.f;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) m = fmaxf(m, s_err[i]);
+      atomicMax(&a.st->err_bits, __float_as_uint(m));
+      if (s_fault) atomicOr(&a.st->fault, s_fault);
+    }
+  }
+}
+
+}  // namespace llb
+
+using namespace llb;
+
+// ------------------------------------------------------------------ host --
+
+namespace {
+
+// e^{2 pi i num/den} rounded once from 80-bit arithmetic, with the angle
+// reduced to the first octant so that cosl/sinl see small arguments.
+double2 unit_root(unsigned long long num, unsigned long long den) {
+  num %= den;
+  // angle fraction f = num/den in [0,1); use 8*num relative to den for octant
+  const long double PI = 3.14159265358979323846264338327950288L;
+  unsigned long long n8 = num * 8;
+  int oct = (int)(n8 / den);
+  long double rem = (long double)(n8 - (unsigned long long)oct * den) / (long double)den;  // [0,1)
+  long double a = rem * PI / 4;  // [0, pi/4)
+  long double c, s;
+  long double ca = cosl(a), sa = sinl(a), cb = cosl(PI / 4 - a), sb = sinl(PI / 4 - a);
+  switch (oct) {
+    case 0: c = ca; s = sa; break;
+    case 1: c = sb; s = cb; break;
+    case 2: c = -sa; s = ca; break;
+    case 3: c = -cb; s = sb; break;
+    case 4: c = -ca; s = -sa; break;
+    case 5: c = -sb; s = -cb; break;
+    case 6: c = sa; s = -ca; break;
+    default: c = cb; s = -sb; break;
+  }
+  return make_double2((double)c, (double)s);
+}
+
+// Radices in the group order of fft_rows: 16, 8, 4, 2, 3, 5, 7.
+bool make_plan(int L, FftPlan &p) {
+  memset(&p, 0, sizeof(p));
+  p.L = L;
+  int m = L, k = 0;
+  static const int rs[] = {16, 8, 4, 2, 3, 5, 7};
+  for (int r : rs)
+    while (m % r == 0) {
+      if (k >= 10) return false;
+      p.radix[k++] = r;
+      m /= r;
+    }
+  p.nst = k;
+  return m == 1;
+}
+
+bool seven_smooth(long long v) {
+  if (v <= 0) return false;
+  for (int p : {2, 3, 5, 7})
+    while (v % p == 0) v /= p;
+  return v == 1;
+}
+
+struct Shape {
+  int W, H, G, T1, T2;
+};
+
+size_t wide_smem(int W, int G) { return sizeof(double2) * (size_t)padded(G * W); }
+size_t tall_smem(int H) { return sizeof(double2) * (size_t)padded(2 * H); }
+const size_t SMEM_MAX = 227 * 1024;
+
+const int TMAX = 256;  // threads per CTA (128 registers per thread)
+
+int round_threads(int need) {
+  int t = (need + 31) / 32 * 32;
+  return std::min(std::max(t, 64), TMAX);
+}
+
+bool shape_ok(long long N, int W, int G, Shape &s) {
+  if (W < 16 || N % W) return false;
+  long long H = N / W;
+  if (W % 2 || H % 2 || H < 16) return false;
+  if (H % G) return false;
+  FftPlan p;
+  if (!make_plan(W, p) || !make_plan((int)H, p)) return false;
+  if (G * W > EPT * TMAX || H > EPT * TMAX) return false;
+  if (wide_smem(W, G) > SMEM_MAX || tall_smem((int)H) > SMEM_MAX) return false;
+  s.W = W;
+  s.H = (int)H;
+  s.G = G;
+  s.T1 = round_threads((G * W + EPT - 1) / EPT);
+  s.T2 = round_threads((int)((2 * H + EPT - 1) / EPT));
+  return true;
+}
+
+// W near sqrt(N); G rows per wide-pass CTA such that a CTA's rows stay
+// within ~100 KB of shared memory (two CTAs per SM).
+bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
+  if (N % 2 || !seven_smooth(N)) return false;
+  std::vector<int> ws;
+  if (t && t->width > 0) ws.push_back(t->width);
+  else {
+    for (long long w = 16; w <= 8192 && w <= N; w += 2)
+      if (N % w == 0) ws.push_back((int)w);
+    double root = sqrt((double)N);
+    std::stable_sort(ws.begin(), ws.end(), [root](int a, int b) {
+      return fabs(log((double)a / root)) < fabs(log((double)b / root));
+    });
+  }
+  for (int w : ws) {
+    std::vector<int> gs;
+    if (t && t->rows_per_cta > 0) gs.push_back(t->rows_per_cta);
+    else
+      for (int g : {8, 4, 2, 1})
+        if (wide_smem(w, g) <= 100 * 1024 || g == 1) gs.push_back(g);
+    for (int g : gs) {
+      Shape s;
+      if (!shape_ok(N, w, g, s)) continue;
+      if (t && t->threads_wide > 0) s.T1 = t->threads_wide;
+      if (t && t->threads_tall > 0) s.T2 = t->threads_tall;
+      if (s.T1 > TMAX || s.T2 > TMAX || s.T1 % 32 || s.T2 % 32 || s.G * s.W > EPT * s.T1 || s.H > EPT * s.T2)
+        continue;
+      out = s;
+      return true;
+    }
+  }
+  return false;
+}
+
+}  // namespace
+
+struct ll_ctx {
+  int device = 0;
+  uint32_t q = 0, n = 0, b = 0, qn = 0;
+  int N = 0;
+  Shape shape{};
+  FftPlan pw{}, ph{};
+  int ts = 0;
+  cudaStream_t stream = nullptr;
+  // device buffers
+  double2 *A = nullptr;
+  int32_t *xint = nullptr;
+  long long *carry = nullptr;
+  uint32_t *flags = nullptr;
+  DevState *st = nullptr;
+  double2 *twW = nullptr, *twH = nullptr, *thi = nullptr, *tlo = nullptr;
+  int32_t *rowE = nullptr, *colF = nullptr;
+  double *rowW = nullptr, *rowWi = nullptr, *colW = nullptr, *colWi = nullptr;
+  // host mirror
+  uint32_t offset = 0;
+  bool digits_current = false;
+  bool started = false;
+  int inject = 0;
+  float pending_err = 0.f;
+  std::string err;
+  TallArgs ta{};
+  WideArgs wa{};
+};
+
+static ll_status cuda_fail(ll_ctx *c, cudaError_t e, const char *what) {
+  if (c) {
+    c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  }
+  return LL_ERR_CUDA;
+}
+
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);       \
+  } while (0)
+
+template <typename T>
+static cudaError_t upload(T **dst, const std::vector<T> &v) {
+  cudaError_t e = cudaMalloc((void **)dst, sizeof(T) * std::max<size_t>(v.size(), 1));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+}
+
+static void free_ctx(ll_ctx *c) {
+  if (!c) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(c->device);
+  void *ptrs[] = {c->A, c->xint, c->carry, c->flags, c->st, c->twW, c->twH, c->thi, c->tlo,
+                  c->rowE, c->colF, c->rowW, c->rowWi, c->colW, c->colWi};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  cudaSetDevice(prev);
+  delete c;
+}
+
+static ll_status build_tables(ll_ctx *ctx) {
+  const int W = ctx->shape.W, H = ctx->shape.H, N = ctx->N;
+  const uint32_t n = ctx->n, b = ctx->b;
+  std::vector<double2> tw(W);
+  for (int e = 0; e < W; ++e) tw[e] = unit_root(e, W);
+  CK(upload(&ctx->twW, tw));
+  tw.resize(H);
+  for (int e = 0; e < H; ++e) tw[e] = unit_root(e, H);
+  CK(upload(&ctx->twH, tw));
+  int ts = 0;
+  while ((1 << (ts + 1)) * (long long)(1 << (ts + 1)) <= (long long)N * 4 && ts < 14) ++ts;
+  ctx->ts = ts;
+  std::vector<double2> lo(1 << ts), hi((N >> ts) + 1);
+  for (int e = 0; e < (1 << ts); ++e) lo[e] = unit_root(e, N);
+  for (size_t e = 0; e < hi.size(); ++e) hi[e] = unit_root((unsigned long long)e << ts, N);
+  CK(upload(&ctx->tlo, lo));
+  CK(upload(&ctx->thi, hi));
+  // weights: word j = 2H*m1 + (2*m2 + t); e_j = (rowE + colF) mod n
+  const long double LN = (long double)n;
+  std::vector<int32_t> rE(2 * H), cF(W);
+  std::vector<double> rW(2 * H), rWi(2 * H), cW(W), cWi(W);
+  for (int jr = 0; jr < 2 * H; ++jr) {
+    long long e = (-(long long)jr * b) % (long long)n;
+    if (e < 0) e += n;
+    rE[jr] = (int32_t)e;
+    rW[jr] = (double)exp2l((long double)e / LN);
+    rWi[jr] = (double)(exp2l(-(long double)e / LN) / (long double)N);
+  }
+  for (int m1 = 0; m1 < W; ++m1) {
+    long long e = (-((long long)2 * H * m1 % (long long)n) * (long long)b) % (long long)n;
+    if (e < 0) e += n;
+    cF[m1] = (int32_t)e;
+    cW[m1] = (double)exp2l((long double)e / LN);
+    cWi[m1] = (double)exp2l(-(long double)e / LN);
+  }
+  CK(upload(&ctx->rowE, rE));
+  CK(upload(&ctx->rowW, rW));
+  CK(upload(&ctx->rowWi, rWi));
+  CK(upload(&ctx->colF, cF));
+  CK(upload(&ctx->colW, cW));
+  CK(upload(&ctx->colWi, cWi));
+  return LL_OK;
+}
+
+extern "C" {
+
+const char *ll_status_string(ll_status s) {
+  switch (s) {
+    case LL_OK: return "ok";
+    case LL_ERR_ARG: return "invalid argument";
+    case LL_ERR_SHAPE: return "unsupported FFT length";
+    case LL_ERR_CUDA: return "CUDA error";
+    case LL_ERR_NOMEM: return "out of memory";
+    case LL_ERR_STATE: return "call out of order";
+    case LL_ERR_TIMEOUT: return "device wait timed out";
+    case LL_ERR_INJECTED: return "injected failure";
+  }
+  return "unknown status";
+}
+
+ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning, ll_ctx **out) {
+  if (!out) return LL_ERR_ARG;
+  *out = nullptr;
+  if (n < 64 || n % 4 || q <= n || q > 0x7fffffffu || (q & 1) == 0) return LL_ERR_ARG;
+  Shape s;
+  if (!choose_shape((long long)n / 2, tuning, s)) return LL_ERR_SHAPE;
+  ll_ctx *ctx = new ll_ctx();
+  ctx->device = device;
+  ctx->q = q;
+  ctx->n = n;
+  ctx->b = q % n;
+  ctx->qn = q / n;
+  ctx->N = (int)(n / 2);
+  ctx->shape = s;
+  if (ctx->qn + 1 > 30) { delete ctx; return LL_ERR_ARG; }
+  make_plan(s.W, ctx->pw);
+  make_plan(s.H, ctx->ph);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { delete ctx; return LL_ERR_CUDA; }
+  ll_status rc = LL_OK;
+  do {
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "stream"); break; }
+    const int ngroups = s.H / s.G;
+    if ((e = cudaMalloc((void **)&ctx->A, sizeof(double2) * (size_t)ctx->N)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&ctx->xint, sizeof(int32_t) * (size_t)n)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&ctx->carry, sizeof(long long) * (size_t)ngroups * s.W)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&ctx->flags, sizeof(uint32_t) * (size_t)ngroups)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&ctx->st, sizeof(DevState))) != cudaSuccess) {
+      rc = e == cudaErrorMemoryAllocation ? LL_ERR_NOMEM : cuda_fail(ctx, e, "cudaMalloc");
+      break;
+    }
+    if ((e = cudaMemset(ctx->flags, 0, sizeof(uint32_t) * (size_t)ngroups)) != cudaSuccess ||
+        (e = cudaMemset(ctx->st, 0, sizeof(DevState))) != cudaSuccess) {
+      rc = cuda_fail(ctx, e, "cudaMemset");
+      break;
+    }
+    rc = build_tables(ctx);
+    if (rc != LL_OK) break;
+    const size_t sw = wide_smem(s.W, s.G), st = tall_smem(s.H);
+    if ((e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_ITER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_REPORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_INIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(tall_kernel<EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess) {
+      rc = cuda_fail(ctx, e, "cudaFuncSetAttribute");
+      break;
+    }
+    TallArgs &ta = ctx->ta;
+    ta.A = ctx->A; ta.twH = ctx->twH; ta.thi = ctx->thi; ta.tlo = ctx->tlo; ta.st = ctx->st;
+    ta.ph = ctx->ph; ta.W = s.W; ta.H = s.H; ta.N = ctx->N; ta.ts = ctx->ts; ta.tmask = (1 << ctx->ts) - 1; ta.q = q;
+    WideArgs &wa = ctx->wa;
+    wa.A = ctx->A; wa.xint = ctx->xint; wa.carry = ctx->carry; wa.flags = ctx->flags; wa.twW = ctx->twW;
+    wa.rowE = ctx->rowE; wa.rowW = ctx->rowW; wa.rowWi = ctx->rowWi;
+    wa.colF = ctx->colF; wa.colW = ctx->colW; wa.colWi = ctx->colWi;
+    wa.st = ctx->st; wa.pw = ctx->pw; wa.W = s.W; wa.H = s.H; wa.G = s.G; wa.ngroups = ngroups;
+    wa.q = q; wa.n = n; wa.b = ctx->b; wa.qn = ctx->qn;
+  } while (0);
+  cudaSetDevice(prev);
+  if (rc != LL_OK) {
+    free_ctx(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return LL_OK;
+}
+
+void ll_destroy(ll_ctx *ctx) { free_ctx(ctx); }
+
+static ll_status launch_init(ll_ctx *ctx) {
+  const Shape &s = ctx->shape;
+  wide_kernel<EPT, WIDE_INIT><<<s.H / s.G, s.T1, wide_smem(s.W, s.G), ctx->stream>>>(ctx->wa);
+  CK(cudaGetLastError());
+  return LL_OK;
+}
+
+ll_status ll_load_digits(ll_ctx *ctx, const int32_t *digits, uint32_t offset) {
+  if (!ctx || !digits || offset >= ctx->q) return LL_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(ctx->xint, digits, sizeof(int32_t) * ctx->n, cudaMemcpyHostToDevice, ctx->stream));
+  DevState hs{};
+  // keep the ticket counter: read it back so that the whole struct can be rewritten
+  CK(cudaMemcpyAsync(&hs, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  hs.offset = offset;
+  hs.err_bits = 0;
+  hs.fault = 0;
+  CK(cudaMemcpyAsync(ctx->st, &hs, sizeof(DevState), cudaMemcpyHostToDevice, ctx->stream));
+  ll_status rc = launch_init(ctx);
+  if (rc != LL_OK) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->offset = offset;
+  ctx->digits_current = true;
+  ctx->started = true;
+  return LL_OK;
+}
+
+ll_status ll_start(ll_ctx *ctx, uint32_t offset) {
+  if (!ctx || offset >= ctx->q) return LL_ERR_ARG;
+  std::vector<int32_t> d(ctx->n, 0);
+  const uint32_t pos = (offset + 2) % ctx->q;
+  const uint32_t w = (uint32_t)(((unsigned long long)pos * ctx->n) / ctx->q);
+  const uint32_t sw = (uint32_t)(((unsigned long long)w * ctx->q + ctx->n - 1) / ctx->n);
+  d[w] = 1 << (pos - sw);
+  return ll_load_digits(ctx, d.data(), offset);
+}
+
+static ll_status launch_iteration(ll_ctx *ctx, bool report) {
+  const Shape &s = ctx->shape;
+  tall_kernel<EPT><<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
+  if (report)
+    wide_kernel<EPT, WIDE_REPORT><<<s.H / s.G, s.T1, wide_smem(s.W, s.G), ctx->stream>>>(ctx->wa);
+  else
+    wide_kernel<EPT, WIDE_ITER><<<s.H / s.G, s.T1, wide_smem(s.W, s.G), ctx->stream>>>(ctx->wa);
+  CK(cudaGetLastError());
+  ctx->offset = (uint32_t)((2ull * ctx->offset) % ctx->q);
+  return LL_OK;
+}
+
+ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
+  if (!ctx) return LL_ERR_ARG;
+  if (!ctx->started) return LL_ERR_STATE;
+  if (ctx->inject > 0) {
+    --ctx->inject;
+    ctx->err = "injected failure";
+    return LL_ERR_INJECTED;
+  }
+  CK(cudaSetDevice(ctx->device));
+  const bool report = (flags & LL_REPORT) != 0;
+  for (uint32_t i = 0; i < iters; ++i) {
+    ll_status rc = launch_iteration(ctx, report && i + 1 == iters);
+    if (rc != LL_OK) return rc;
+  }
+  if (iters) ctx->digits_current = report;
+  if (flags & (LL_REPORT | LL_ERRCHK)) {
+    DevState hs{};
+    CK(cudaMemcpyAsync(&hs, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const uint32_t zero[2] = {0, 0};
+    CK(cudaMemcpyAsync(&ctx->st->err_bits, zero, sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    float e;
+    memcpy(&e, &hs.err_bits, sizeof(float));
+    if (max_err) *max_err = e;
+    if (hs.offset != ctx->offset) {
+      ctx->err = "device offset diverged from host mirror";
+      return LL_ERR_STATE;
+    }
+    if (hs.fault & 1u) {
+      ctx->err = "wide pass: carry wait timed out";
+      return LL_ERR_TIMEOUT;
+    }
+    if (hs.fault & 2u) {
+      ctx->err = "wide pass: carry out of range (roundoff far above 0.5)";
+      if (max_err) *max_err = 1.0f;
+    }
+  }
+  return LL_OK;
+}
+
+ll_status ll_sync(ll_ctx *ctx) {
+  if (!ctx) return LL_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return LL_OK;
+}
+
+ll_status ll_read_digits(ll_ctx *ctx, int32_t *digits, uint32_t *offset) {
+  if (!ctx || !digits) return LL_ERR_ARG;
+  if (!ctx->digits_current) return LL_ERR_STATE;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(digits, ctx->xint, sizeof(int32_t) * ctx->n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (offset) *offset = ctx->offset;
+  return LL_OK;
+}
+
+ll_status ll_res64(ll_ctx *ctx, uint64_t *res64) {
+  if (!ctx || !res64) return LL_ERR_ARG;
+  std::vector<int32_t> d(ctx->n);
+  uint32_t off = 0;
+  ll_status rc = ll_read_digits(ctx, d.data(), &off);
+  if (rc != LL_OK) return rc;
+  *res64 = ll_digits_res64(d.data(), ctx->q, ctx->n, off);
+  return LL_OK;
+}
+
+uint32_t ll_exponent(const ll_ctx *ctx) { return ctx ? ctx->q : 0; }
+uint32_t ll_fft_length(const ll_ctx *ctx) { return ctx ? ctx->n : 0; }
+uint32_t ll_offset(const ll_ctx *ctx) { return ctx ? ctx->offset : 0; }
+void *ll_stream(const ll_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+void ll_shape(const ll_ctx *ctx, int32_t *width, int32_t *height, int32_t *rows_per_cta, int32_t *threads_wide,
+              int32_t *threads_tall) {
+  if (!ctx) return;
+  if (width) *width = ctx->shape.W;
+  if (height) *height = ctx->shape.H;
+  if (rows_per_cta) *rows_per_cta = ctx->shape.G;
+  if (threads_wide) *threads_wide = ctx->shape.T1;
+  if (threads_tall) *threads_tall = ctx->shape.T2;
+}
+const char *ll_last_error(const ll_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+void ll_debug_inject_failure(ll_ctx *ctx, int32_t count) {
+  if (ctx) ctx->inject = count;
+}
+
+ll_status ll_debug_launch(ll_ctx *ctx, int32_t which) {
+  if (!ctx || !ctx->started) return LL_ERR_STATE;
+  CK(cudaSetDevice(ctx->device));
+  const Shape &s = ctx->shape;
+  if (which == 0) {
+    tall_kernel<EPT><<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
+    ctx->offset = (uint32_t)((2ull * ctx->offset) % ctx->q);
+  } else {
+    wide_kernel<EPT, WIDE_ITER><<<s.H / s.G, s.T1, wide_smem(s.W, s.G), ctx->stream>>>(ctx->wa);
+  }
+  ctx->digits_current = false;
+  CK(cudaGetLastError());
+  return LL_OK;
+}
+
+int32_t ll_length_supported(uint32_t n) {
+  if (n < 64 || n % 4) return 0;
+  Shape s;
+  return choose_shape((long long)n / 2, nullptr, s) ? 1 : 0;
+}
+
+}  // extern "C"

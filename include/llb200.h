@@ -1,0 +1,147 @@
+/*
+ * llb200.h -- C ABI of the B200 Lucas-Lehmer engine (libllb200.so).
+ *
+ * The engine replaces the per-iteration squaring of CUDALucas v2.06:
+ *   float lucas_square(int q, int n, int iter, int last, int *offset,
+ *                      float *maxerr, int error_flag)      CUDALucas.cu:1869
+ * which works on module-global device buffers set up by init_lucas
+ * (CUDALucas.cu:1344) and torn down by close_lucas (CUDALucas.cu:1415).
+ * Here every exponent under test is an opaque context that owns its device
+ * buffers and its CUDA stream, so several contexts can live in one process.
+ * No function calls exit(); every failure is a status code.
+ *
+ * Plain C types only: pointers are host pointers unless stated otherwise.
+ */
+#ifndef LLB200_H
+#define LLB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  LL_OK = 0,
+  LL_ERR_ARG = 1,       /* bad argument (exponent, length, pointer, size)   */
+  LL_ERR_SHAPE = 2,     /* no supported FFT decomposition for this length   */
+  LL_ERR_CUDA = 3,      /* CUDA runtime error (see ll_last_error)           */
+  LL_ERR_NOMEM = 4,     /* device or host allocation failed                 */
+  LL_ERR_STATE = 5,     /* call out of order (e.g. digits not current)      */
+  LL_ERR_TIMEOUT = 6,   /* a bounded device-side wait gave up               */
+  LL_ERR_INJECTED = 7   /* failure injected through ll_debug_inject_failure */
+} ll_status;
+
+/* Flags of ll_step.  LL_REPORT mirrors bit 0 of lucas_square's error_flag
+ * (digits written on the last iteration, CUDALucas.cu:1929); LL_ERRCHK
+ * mirrors bit 1 (max roundoff error read back, CUDALucas.cu:1973-1978). */
+#define LL_REPORT 1u
+#define LL_ERRCHK 2u
+
+typedef struct ll_ctx ll_ctx;
+
+/* Optional launch shape.  Zero fields are chosen by the engine. */
+typedef struct {
+  int32_t width;        /* W: row-transform length (complex elements)       */
+  int32_t rows_per_cta; /* G: rows handled by one CTA of the wide pass      */
+  int32_t threads_wide; /* threads per CTA of the wide pass                 */
+  int32_t threads_tall; /* threads per CTA of the tall pass                 */
+  int32_t graph_iters;  /* iterations captured per CUDA graph (0 = auto)    */
+  int32_t reserved[3];
+} ll_tuning;
+
+/* Creates a context for exponent q at FFT length n (FP64 words) on `device`.
+ * Replaces alloc_gpu_mem + write_gpu_data (CUDALucas.cu:1096, :1125).
+ * n must be even, n/2 must factor into a supported W x H split, q > n. */
+ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
+                    ll_ctx **out);
+
+/* Releases the context (CUDALucas.cu:1415 close_lucas). NULL is a no-op. */
+void ll_destroy(ll_ctx *ctx);
+
+/* Starts a fresh test: s0 = 4 stored as 4*2^offset (CUDALucas.cu:1254-1262
+ * init_x with the offset given instead of rand() % q). */
+ll_status ll_start(ll_ctx *ctx, uint32_t offset);
+
+/* Loads n balanced digits (word j holds floor(q/n) or floor(q/n)+1 bits) of
+ * x = s * 2^offset mod 2^q-1 (CUDALucas.cu:1254-1278 init_x/apply_weights
+ * on a resumed test). */
+ll_status ll_load_digits(ll_ctx *ctx, const int32_t *digits, uint32_t offset);
+
+/* Runs `iters` LL iterations (iters x lucas_square, CUDALucas.cu:1869).
+ * LL_REPORT: digits of the final state become readable by ll_read_digits.
+ * LL_REPORT or LL_ERRCHK: waits for the GPU and stores the max roundoff
+ * error seen since the last read in *max_err (may be NULL).  Without either
+ * flag the call only enqueues work and returns. */
+ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err);
+
+/* Copies the n digits written by the last LL_REPORT step (or the last
+ * load/start) and the matching offset (CUDALucas.cu:2963 g_xint D2H). */
+ll_status ll_read_digits(ll_ctx *ctx, int32_t *digits, uint32_t *offset);
+
+/* Res64 of the current state (find_residue, CUDALucas.cu:1491); requires
+ * current digits like ll_read_digits. */
+ll_status ll_res64(ll_ctx *ctx, uint64_t *res64);
+
+/* Waits for all queued work of the context. */
+ll_status ll_sync(ll_ctx *ctx);
+
+/* Properties of a context. */
+uint32_t ll_exponent(const ll_ctx *ctx);
+uint32_t ll_fft_length(const ll_ctx *ctx);
+uint32_t ll_offset(const ll_ctx *ctx);
+void *ll_stream(const ll_ctx *ctx);           /* the context's cudaStream_t */
+void ll_shape(const ll_ctx *ctx, int32_t *width, int32_t *height,
+              int32_t *rows_per_cta, int32_t *threads_wide, int32_t *threads_tall);
+const char *ll_last_error(const ll_ctx *ctx); /* text of the last failure   */
+const char *ll_status_string(ll_status s);
+
+/* Test hook (CUDALucas.cu:2938-2950 handles a CUDA error from lucas_square
+ * by resetting and restarting from the last checkpoint): the next `count`
+ * ll_step calls return LL_ERR_INJECTED without touching the device. */
+void ll_debug_inject_failure(ll_ctx *ctx, int32_t count);
+
+/* Launches only the tall pass (square) or only the wide pass (carry) of one
+ * iteration; used to time and profile the passes separately. */
+ll_status ll_debug_launch(ll_ctx *ctx, int32_t which);
+
+/* ------------------------------------------------------------------------
+ * Host helpers (no GPU needed).  Word j of an n-word representation of
+ * 2^q-1 has floor(q/n)+1 bits iff ((-j*(q mod n)) mod n) < (q mod n).
+ * ---------------------------------------------------------------------- */
+
+/* Res64 of x*2^-offset mod 2^q-1 from any digit vector (exact; the digits
+ * need not be balanced).  Same value as find_residue, CUDALucas.cu:1491. */
+uint64_t ll_digits_res64(const int32_t *digits, uint32_t q, uint32_t n, uint32_t offset);
+
+/* Canonicalises digits in place to 0 <= d_j < 2^bits_j with value in
+ * [0, 2^q-1); returns 1 if the value is 0 mod 2^q-1 (standardize_digits,
+ * CUDALucas.cu:1465). */
+int32_t ll_digits_standardize(int32_t *digits, uint32_t q, uint32_t n);
+
+/* pack_bits / unpack_bits / balance_digits, CUDALucas.cu:1594, :1285, :1313.
+ * packed has (q+31)/32 words. */
+void ll_pack_bits(const int32_t *digits, uint32_t *packed, uint32_t q, uint32_t n);
+void ll_unpack_bits(const uint32_t *packed, int32_t *digits, uint32_t q, uint32_t n);
+void ll_balance_digits(int32_t *digits, uint32_t q, uint32_t n);
+
+/* checkpoint_checksum (CRC-32 style, poly 0x04C11DB7, CUDALucas.cu:1712) and
+ * the additive ch_sum (CUDALucas.cu:1735). */
+uint32_t ll_checkpoint_checksum(const void *bytes, size_t len);
+uint32_t ll_additive_checksum(const uint32_t *words, size_t count);
+
+/* FFT-length policy of CUDALucas (init_ffts / choose_fft_length,
+ * CUDALucas.cu:947-1068) with the built-in 7-smooth table.
+ * ll_fft_bounds gives the exponent's [lb, ub] word-count bounds;
+ * ll_choose_fft_length returns the smallest table length >= max(lb, want)
+ * that the engine supports and that is <= ub, or 0 if none. */
+void ll_fft_bounds(uint32_t q, uint32_t *lb, uint32_t *ub);
+uint32_t ll_choose_fft_length(uint32_t q, uint32_t want);
+int32_t ll_fft_table(uint32_t *lengths, int32_t max_count);
+int32_t ll_length_supported(uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LLB200_H */

@@ -1,0 +1,27 @@
+"""Loaders for the committed golden fixtures in tests/golden/."""
+import json
+import os
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def kats(table=None):
+    d = json.load(open(os.path.join(HERE, "kat_res64.json")))
+    names = [table] if table else ["tests", "testl"]
+    out = []
+    for nm in names:
+        out += [(p, int(r, 16)) for p, r in d[nm]["entries"]]
+    return out
+
+
+def exact_entries():
+    d = json.load(open(os.path.join(HERE, "exact_res64.json")))
+    return [(p, k, int(r, 16)) for p, k, r in d["entries"]]
+
+
+def large_entries():
+    path = os.path.join(HERE, "large_res64.json")
+    if not os.path.exists(path):
+        return []
+    d = json.load(open(path))
+    return [(p, k, int(r, 16)) for p, k, r in d["entries"]]

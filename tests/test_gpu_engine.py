@@ -1,0 +1,181 @@
+"""GPU parity tests: the CUDA engine (through the C ABI) against the oracle.
+
+Res64 is compared bit-exactly; digit vectors are compared after
+canonicalisation (exact value mod 2^q-1), and against the numpy model of the
+engine's own carry scheme bit for bit.  The roundoff error is checked against
+the reference's 0.40 limit (CUDALucas.cu:2765) and against the oracle's error
+within a factor of 2 (FFT rounding differs between implementations)."""
+import numpy as np
+import pytest
+
+import cudalucas_b200 as cl
+import ibdwt_model
+from golden_data import kats, large_entries
+from oracle import exact
+from oracle.binding import Oracle
+
+pytestmark = pytest.mark.gpu
+KAT = dict(kats())
+
+
+def engine_run(q, n, offset, k, **tuning):
+    with cl.LLContext(q, n, tuning=tuning or None) as c:
+        c.start(offset)
+        err = c.step(k, report=True)
+        d, off = c.read_digits()
+        return d, off, err, c.shape
+
+
+@pytest.mark.parametrize("q,n", [(86243, 4096), (132049, 7168), (216091, 12288), (216091, 14336),
+                                 (756839, 40960), (1257787, 65536), (2976221, 163840), (6972593, 393216)])
+def test_parity_with_oracle(q, n):
+    k = 60
+    off = (q * 5) // 11
+    d, o_off, err, shape = engine_run(q, n, off, k)
+    o = Oracle(q, n)
+    o.start(off)
+    oerr = o.step(k)
+    od = o.digits()
+    assert o_off == o.offset
+    sd, _ = cl.standardize(d, q, n)
+    so, _ = cl.standardize(od, q, n)
+    assert np.array_equal(sd, so)
+    assert cl.digits_res64(d, q, n, o_off) == o.res64()
+    assert err < 0.4
+    assert err <= 2 * oerr + 1e-3 and oerr <= 2 * err + 1e-3, (err, oerr)
+
+
+@pytest.mark.parametrize("q,n", [(86243, 4096), (216091, 12288), (1257787, 65536)])
+def test_digits_match_engine_model_bit_for_bit(q, n):
+    off = q // 7
+    d, _, _, shape = engine_run(q, n, off, 25)
+    m = ibdwt_model.Model(q, n, shape["W"])
+    m.start(off)
+    for _ in range(25):
+        m.iterate()
+    assert np.array_equal(d.astype(np.int64), m.digits)
+
+
+def test_report_split_equals_single_run():
+    q, n = 132049, 7168
+    with cl.LLContext(q, n) as c:
+        c.start(3)
+        c.step(40, report=True)
+        c.step(60, report=True)
+        d1, o1 = c.read_digits()
+    d2, o2, _, _ = engine_run(q, n, 3, 100)
+    assert o1 == o2
+    assert np.array_equal(cl.standardize(d1, q, n)[0], cl.standardize(d2, q, n)[0])
+
+
+def test_load_digits_resume_equals_continuous():
+    q, n = 216091, 12288
+    with cl.LLContext(q, n) as c:
+        c.start(1000)
+        c.step(500, report=True)
+        mid, off = c.read_digits()
+    with cl.LLContext(q, n) as c:
+        c.load_digits(cl.balance_digits(cl.standardize(mid, q, n)[0], q, n), off)
+        c.step(500, report=True)
+        r_resumed = c.res64()
+    assert r_resumed == exact.res64(q, 1000)
+
+
+@pytest.mark.parametrize("p,r", kats("tests"))
+def test_selftest_short_table(p, r):
+    n = cl.choose_fft_length(p)
+    with cl.LLContext(p, n) as c:
+        c.start((p * 3) // 17)
+        err = c.step(10000, report=True)
+        assert c.res64() == r
+        assert err < 0.4
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("p,r", kats("testl"))
+def test_selftest_long_table(p, r):
+    n = cl.choose_fft_length(p)
+    with cl.LLContext(p, n) as c:
+        c.start((p * 3) // 17)
+        err = c.step(10000, report=True)
+        assert c.res64() == r
+        assert err < 0.4
+
+
+def test_c1_full_test_216091_is_prime():
+    q, n = 216091, 12288
+    with cl.LLContext(q, n) as c:
+        c.start(0)
+        done, maxerr = 0, 0.0
+        while done < q - 2:
+            k = min(10000, q - 2 - done)
+            maxerr = max(maxerr, c.step(k, report=True))
+            done += k
+            if done == 10000:
+                assert c.res64() == KAT[q]
+        assert c.res64() == 0
+        assert maxerr < 0.4
+
+
+def test_c2_3200k_kat_at_10000():
+    q, n = 57885161, 3276800
+    checks = {k: r for p, k, r in large_entries() if p == q}
+    with cl.LLContext(q, n) as c:
+        c.start(0)
+        done = 0
+        for k in sorted(list(checks) + [10000]):
+            err = c.step(k - done, report=True)
+            done = k
+            assert err < 0.4
+            assert c.res64() == (KAT[q] if k == 10000 else checks[k])
+
+
+def test_c3_18432k_matches_exact():
+    q, n = 332192831, 18874368
+    checks = {k: r for p, k, r in large_entries() if p == q}
+    if not checks:
+        pytest.skip("large fixture not generated")
+    with cl.LLContext(q, n) as c:
+        c.start(0)
+        done = 0
+        for k in sorted(checks):
+            err = c.step(k - done, report=True)
+            done = k
+            assert err < 0.4
+            assert c.res64() == checks[k]
+
+
+def test_independent_contexts_interleaved():
+    a = cl.LLContext(86243, 4096)
+    b = cl.LLContext(132049, 7168)
+    a.start(11)
+    b.start(22)
+    for _ in range(5):
+        a.step(200)
+        b.step(200)
+    a.step(0, report=True)
+    ra = a.step(1, report=True) and a.res64()
+    rb = b.step(1, report=True) and b.res64()
+    a.close()
+    b.close()
+    assert ra == exact.res64(86243, 1001)
+    assert rb == exact.res64(132049, 1001)
+
+
+def test_injected_failure_is_reported_and_recoverable():
+    with cl.LLContext(86243, 4096) as c:
+        c.start(0)
+        c.inject_failure(1)
+        with pytest.raises(cl.LLError) as ei:
+            c.step(10)
+        assert ei.value.status == 7
+        c.step(100, report=True)
+        assert c.res64() == exact.res64(86243, 100)
+
+
+def test_read_digits_requires_report():
+    with cl.LLContext(86243, 4096) as c:
+        c.start(0)
+        c.step(5)
+        with pytest.raises(cl.LLError):
+            c.read_digits()
