@@ -21,7 +21,7 @@ def nvcc():
 
 def build(verbose=False, extra=()):
     srcs = [os.path.join(SRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(SRC, "fft_device.cuh"), os.path.join(ROOT, "include", "llb200.h")]
+    deps = srcs + [os.path.join(SRC, h) for h in os.listdir(SRC) if h.endswith(".cuh")] + [os.path.join(ROOT, "include", "llb200.h")]
     if os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(d) for d in deps) and not extra:
         return OUT
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--shared", "-Xcompiler", "-fPIC",
@@ -33,8 +33,30 @@ def build(verbose=False, extra=()):
     return OUT
 
 
+CLI_SRC = os.path.join(HERE, "host", "llucas.cpp")
+CLI_OUT = os.path.join(HERE, "bin", "llucas")
+
+
+def build_cli(verbose=False):
+    """The command-line tester (C++ host over the C ABI), linked to the
+    in-tree libllb200.so through an $ORIGIN-relative rpath."""
+    build()
+    deps = [CLI_SRC, os.path.join(ROOT, "include", "llb200.h"), OUT]
+    if os.path.exists(CLI_OUT) and all(os.path.getmtime(CLI_OUT) >= os.path.getmtime(d) for d in deps):
+        return CLI_OUT
+    os.makedirs(os.path.dirname(CLI_OUT), exist_ok=True)
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), "-o", CLI_OUT + ".tmp",
+           CLI_SRC, "-L", HERE, "-lllb200", "-Wl,-rpath,$ORIGIN/.."]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.check_call(cmd)
+    os.replace(CLI_OUT + ".tmp", CLI_OUT)
+    return CLI_OUT
+
+
 if __name__ == "__main__":
     extra = []
     if "--ptxas-v" in sys.argv:
         extra += ["-Xptxas", "-v"]
     print(build(verbose=True, extra=extra))
+    print(build_cli(verbose=True))

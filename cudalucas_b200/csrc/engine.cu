@@ -33,11 +33,13 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/llb200.h"
 #include "fft_device.cuh"
+#include "twiddle_consts.cuh"
 
 namespace llb {
 
@@ -344,6 +346,58 @@ __global__ void __launch_bounds__(256) wide_kernel(WideArgs a) {
   }
 }
 
+#include "kernels_static.cuh"
+
+// Registry of compile-time specialised kernels, by row length.
+struct StaticWide {
+  int L, G;
+  void (*iter)(WideArgs);
+  void (*report)(WideArgs);
+  void (*init)(WideArgs);
+};
+struct StaticTall {
+  int L;
+  void (*run)(TallArgs);
+};
+
+#define LLB_WIDE(LIST, G) \
+  {LIST::L, G, wide_static<LIST, G, WIDE_ITER>, wide_static<LIST, G, WIDE_REPORT>, wide_static<LIST, G, WIDE_INIT>}
+#define LLB_TALL(LIST) {LIST::L, tall_static<LIST>}
+
+using L512 = RList<16, 2, 16>;
+using L768 = RList<16, 3, 16>;
+using L1024 = RList<16, 4, 16>;
+using L1280 = RList<16, 5, 16>;
+using L1536 = RList<16, 6, 16>;
+using L1792 = RList<16, 7, 16>;
+using L2048 = RList<16, 8, 16>;
+using L2304 = RList<16, 9, 16>;
+using L2560 = RList<16, 10, 16>;
+using L3072 = RList<16, 12, 16>;
+using L3584 = RList<16, 14, 16>;
+using L4096 = RList<16, 16, 16>;
+
+static const StaticWide kWide[] = {
+    LLB_WIDE(L512, 4),  LLB_WIDE(L768, 4),  LLB_WIDE(L1024, 2), LLB_WIDE(L1280, 2),
+    LLB_WIDE(L1536, 2), LLB_WIDE(L1792, 2), LLB_WIDE(L2048, 2), LLB_WIDE(L2304, 2),
+    LLB_WIDE(L2560, 1), LLB_WIDE(L3072, 1), LLB_WIDE(L3584, 1), LLB_WIDE(L4096, 1),
+};
+static const StaticTall kTall[] = {
+    LLB_TALL(L512),  LLB_TALL(L768),  LLB_TALL(L1024), LLB_TALL(L1280), LLB_TALL(L1536), LLB_TALL(L1792),
+    LLB_TALL(L2048), LLB_TALL(L2304), LLB_TALL(L2560), LLB_TALL(L3072), LLB_TALL(L3584), LLB_TALL(L4096),
+};
+
+static const StaticWide *find_wide(int L) {
+  for (const auto &k : kWide)
+    if (k.L == L) return &k;
+  return nullptr;
+}
+static const StaticTall *find_tall(int L) {
+  for (const auto &k : kTall)
+    if (k.L == L) return &k;
+  return nullptr;
+}
+
 }  // namespace llb
 
 using namespace llb;
@@ -402,6 +456,8 @@ bool seven_smooth(long long v) {
 
 struct Shape {
   int W, H, G, T1, T2;
+  const StaticWide *sw = nullptr;  // specialised kernels, when both exist
+  const StaticTall *st = nullptr;
 };
 
 size_t wide_smem(int W, int G) { return sizeof(double2) * (size_t)padded(G * W); }
@@ -436,6 +492,35 @@ bool shape_ok(long long N, int W, int G, Shape &s) {
 // within ~100 KB of shared memory (two CTAs per SM).
 bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
   if (N % 2 || !seven_smooth(N)) return false;
+  // compile-time specialised kernels for both passes, W closest to sqrt(N)
+  if (!(t && (t->rows_per_cta > 0 || t->threads_wide > 0 || t->threads_tall > 0 || t->reserved[0]))) {
+    const StaticWide *bw = nullptr;
+    const StaticTall *bt = nullptr;
+    double best = 1e30;
+    for (const auto &w : kWide) {
+      if (N % w.L) continue;
+      if (t && t->width > 0 && t->width != w.L) continue;
+      const long long H = N / w.L;
+      const StaticTall *tt = find_tall((int)H);
+      if (!tt || H % w.G) continue;
+      const double d = fabs(log((double)w.L / sqrt((double)N)));
+      if (d < best) {
+        best = d;
+        bw = &w;
+        bt = tt;
+      }
+    }
+    if (bw) {
+      out.W = bw->L;
+      out.H = (int)(N / bw->L);
+      out.G = bw->G;
+      out.T1 = bw->G * (bw->L / 16);
+      out.T2 = 2 * (out.H / 16);
+      out.sw = bw;
+      out.st = bt;
+      return true;
+    }
+  }
   std::vector<int> ws;
   if (t && t->width > 0) ws.push_back(t->width);
   else {
@@ -631,13 +716,35 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
     }
     rc = build_tables(ctx);
     if (rc != LL_OK) break;
-    const size_t sw = wide_smem(s.W, s.G), st = tall_smem(s.H);
-    if ((e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_ITER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_REPORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_INIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(tall_kernel<EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess) {
-      rc = cuda_fail(ctx, e, "cudaFuncSetAttribute");
-      break;
+    // The dynamic shared-memory limit is a per-function (not per-context)
+    // attribute: raise it to the largest size any context has needed.
+    {
+      static std::mutex mu;
+      static size_t max_sw = 0, max_st = 0;
+      std::lock_guard<std::mutex> lock(mu);
+      const size_t sw = std::max(max_sw, wide_smem(s.W, s.G)), st = std::max(max_st, tall_smem(s.H));
+      if ((e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_ITER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
+          (e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_REPORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
+          (e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_INIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
+          (e = cudaFuncSetAttribute(tall_kernel<EPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess) {
+        rc = cuda_fail(ctx, e, "cudaFuncSetAttribute");
+        break;
+      }
+      for (const auto &k : kWide)
+        if ((e = cudaFuncSetAttribute(k.iter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(k.report, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(k.init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess)
+          break;
+      for (const auto &k : kTall)
+        if (e == cudaSuccess &&
+            (e = cudaFuncSetAttribute(k.run, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess)
+          break;
+      if (e != cudaSuccess) {
+        rc = cuda_fail(ctx, e, "cudaFuncSetAttribute (static)");
+        break;
+      }
+      max_sw = sw;
+      max_st = st;
     }
     TallArgs &ta = ctx->ta;
     ta.A = ctx->A; ta.twH = ctx->twH; ta.thi = ctx->thi; ta.tlo = ctx->tlo; ta.st = ctx->st;
@@ -660,9 +767,29 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
 
 void ll_destroy(ll_ctx *ctx) { free_ctx(ctx); }
 
-static ll_status launch_init(ll_ctx *ctx) {
+static void launch_wide(ll_ctx *ctx, int mode) {
   const Shape &s = ctx->shape;
-  wide_kernel<EPT, WIDE_INIT><<<s.H / s.G, s.T1, wide_smem(s.W, s.G), ctx->stream>>>(ctx->wa);
+  const size_t sm = wide_smem(s.W, s.G);
+  if (s.sw) {
+    void (*k)(WideArgs) = mode == WIDE_INIT ? s.sw->init : mode == WIDE_REPORT ? s.sw->report : s.sw->iter;
+    k<<<s.H / s.G, s.T1, sm, ctx->stream>>>(ctx->wa);
+  } else if (mode == WIDE_INIT) {
+    wide_kernel<EPT, WIDE_INIT><<<s.H / s.G, s.T1, sm, ctx->stream>>>(ctx->wa);
+  } else if (mode == WIDE_REPORT) {
+    wide_kernel<EPT, WIDE_REPORT><<<s.H / s.G, s.T1, sm, ctx->stream>>>(ctx->wa);
+  } else {
+    wide_kernel<EPT, WIDE_ITER><<<s.H / s.G, s.T1, sm, ctx->stream>>>(ctx->wa);
+  }
+}
+
+static void launch_tall(ll_ctx *ctx) {
+  const Shape &s = ctx->shape;
+  if (s.st) s.st->run<<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
+  else tall_kernel<EPT><<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
+}
+
+static ll_status launch_init(ll_ctx *ctx) {
+  launch_wide(ctx, WIDE_INIT);
   CK(cudaGetLastError());
   return LL_OK;
 }
@@ -699,12 +826,8 @@ ll_status ll_start(ll_ctx *ctx, uint32_t offset) {
 }
 
 static ll_status launch_iteration(ll_ctx *ctx, bool report) {
-  const Shape &s = ctx->shape;
-  tall_kernel<EPT><<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
-  if (report)
-    wide_kernel<EPT, WIDE_REPORT><<<s.H / s.G, s.T1, wide_smem(s.W, s.G), ctx->stream>>>(ctx->wa);
-  else
-    wide_kernel<EPT, WIDE_ITER><<<s.H / s.G, s.T1, wide_smem(s.W, s.G), ctx->stream>>>(ctx->wa);
+  launch_tall(ctx);
+  launch_wide(ctx, report ? WIDE_REPORT : WIDE_ITER);
   CK(cudaGetLastError());
   ctx->offset = (uint32_t)((2ull * ctx->offset) % ctx->q);
   return LL_OK;
@@ -798,12 +921,11 @@ void ll_debug_inject_failure(ll_ctx *ctx, int32_t count) {
 ll_status ll_debug_launch(ll_ctx *ctx, int32_t which) {
   if (!ctx || !ctx->started) return LL_ERR_STATE;
   CK(cudaSetDevice(ctx->device));
-  const Shape &s = ctx->shape;
   if (which == 0) {
-    tall_kernel<EPT><<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
+    launch_tall(ctx);
     ctx->offset = (uint32_t)((2ull * ctx->offset) % ctx->q);
   } else {
-    wide_kernel<EPT, WIDE_ITER><<<s.H / s.G, s.T1, wide_smem(s.W, s.G), ctx->stream>>>(ctx->wa);
+    launch_wide(ctx, WIDE_ITER);
   }
   ctx->digits_current = false;
   CK(cudaGetLastError());

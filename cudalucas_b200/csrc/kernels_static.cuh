@@ -1,0 +1,372 @@
+// Compile-time specialised tall/wide passes for row lengths L = 16 * M.
+//
+// Same mathematics and data layout as the generic kernels in engine.cu, but
+// the radix list of the row transform is a template parameter, so every
+// index, stride and loop bound is a constant, and the first radix is 16:
+//  * a row of L elements is handled by TR = L/16 threads;
+//  * the inverse transform runs the radix list backwards, so its last stage
+//    (radix 16) leaves element m1 = t + r*TR of the row in register r of
+//    thread t -- exactly the inputs of the forward transform's first stage.
+//    The wide pass therefore rounds, carries and reweights in registers
+//    between the two transforms, with no shared-memory round trip;
+//  * the tall pass loads its first stage straight from HBM and stores its
+//    last stage straight to HBM (both coalesced along the column).
+// Included from engine.cu inside namespace llb, after the shared helpers.
+
+template <int... Rs>
+struct RList {
+  static constexpr int N = sizeof...(Rs);
+  static constexpr int a[N] = {Rs...};
+  static constexpr int L = (Rs * ... * 1);
+};
+
+// Composite DFT of radix P*Q in registers: DFT_P over c1 for every c2,
+// twiddles w_R^(c2*k1), DFT_Q over c2 for every k1.  Output k1 + P*k2 is
+// left in v[Q*k1 + k2].
+template <int P, int Q, int SIGN>
+__device__ __forceinline__ void dft_pq(double2 *v) {
+  constexpr int R = P * Q;
+#pragma unroll
+  for (int c2 = 0; c2 < Q; ++c2) {
+    double2 w[P];
+#pragma unroll
+    for (int c1 = 0; c1 < P; ++c1) w[c1] = v[Q * c1 + c2];
+    dft<P, SIGN>(w);
+#pragma unroll
+    for (int k1 = 0; k1 < P; ++k1) {
+      double2 y = w[out_slot<P>(k1)];
+      if (c2 != 0 && k1 != 0) {
+        double2 t = wconst<R>(c2 * k1);
+        y = SIGN > 0 ? cmul(y, t) : cmulc(y, t);
+      }
+      v[Q * k1 + c2] = y;
+    }
+  }
+#pragma unroll
+  for (int k1 = 0; k1 < P; ++k1) {
+    double2 w[Q];
+#pragma unroll
+    for (int c2 = 0; c2 < Q; ++c2) w[c2] = v[Q * k1 + c2];
+    dft<Q, SIGN>(w);
+#pragma unroll
+    for (int k2 = 0; k2 < Q; ++k2) v[Q * k1 + k2] = w[out_slot<Q>(k2)];
+  }
+}
+
+template <int R>
+struct Split {  // factor P*Q of a composite radix (P = 0: prime kernel)
+  static constexpr int P = R == 6 ? 2 : R == 9 ? 3 : R == 10 ? 2 : R == 12 ? 4 : R == 14 ? 2 : R == 20 ? 4 : 0;
+  static constexpr int Q = P ? R / P : 0;
+};
+
+template <int R, int SIGN>
+__device__ __forceinline__ void sdft(double2 *v) {
+  if constexpr (Split<R>::P) dft_pq<Split<R>::P, Split<R>::Q, SIGN>(v);
+  else dft<R, SIGN>(v);
+}
+
+template <int R>
+__device__ __forceinline__ constexpr int sslot(int r) {
+  if constexpr (Split<R>::P) return Split<R>::Q * (r % Split<R>::P) + r / Split<R>::P;
+  else return out_slot<R>(r);
+}
+
+// One Stockham stage of every row of the CTA, in place in shared memory.
+// Thread t of a row handles butterflies t, t+TR, ... (a guard skips the
+// tail when L/R is not a multiple of TR).
+template <int L, int R, int NS, int SIGN, int TR>
+__device__ __forceinline__ void sstage(double2 *s, const double2 *__restrict__ tw, int row, int t) {
+  constexpr int M = L / R;
+  constexpr int NB = (M + TR - 1) / TR;
+  constexpr int STEP = L / (NS * R);
+  double2 v[NB][R];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const int j = t + b * TR;
+    if (M % TR == 0 || j < M) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = s[pad(row * L + j + r * M)];
+      if constexpr (NS > 1) {
+        const int k = j % NS;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const double2 w = __ldg(&tw[r * k * STEP]);
+          v[b][r] = SIGN > 0 ? cmul(v[b][r], w) : cmulc(v[b][r], w);
+        }
+      }
+      sdft<R, SIGN>(v[b]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const int j = t + b * TR;
+    if (M % TR == 0 || j < M) {
+      const int k = j % NS;
+      const int ob = row * L + (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[pad(ob + r * NS)] = v[b][sslot<R>(r)];
+    }
+  }
+  __syncthreads();
+}
+
+// forward stages [I, E) (radix a[I], NS = a[0]*...*a[I-1])
+template <class P, int I, int E, int NS, int TR>
+__device__ __forceinline__ void fwd_stages(double2 *s, const double2 *__restrict__ tw, int row, int t) {
+  if constexpr (I < E) {
+    constexpr int R = P::a[I];
+    sstage<P::L, R, NS, +1, TR>(s, tw, row, t);
+    fwd_stages<P, I + 1, E, NS * R, TR>(s, tw, row, t);
+  }
+}
+
+// inverse stages [I, E) of the reversed list (radix a[N-1-I])
+template <class P, int I, int E, int NS, int TR>
+__device__ __forceinline__ void inv_stages(double2 *s, const double2 *__restrict__ tw, int row, int t) {
+  if constexpr (I < E) {
+    constexpr int R = P::a[P::N - 1 - I];
+    sstage<P::L, R, NS, -1, TR>(s, tw, row, t);
+    inv_stages<P, I + 1, E, NS * R, TR>(s, tw, row, t);
+  }
+}
+
+// Forward first stage (radix 16, no twiddle) from registers x[t + r*TR].
+template <int L, int TR>
+__device__ __forceinline__ void first_stage_from_regs(double2 *s, double2 *v, int row, int t) {
+  dft<16, +1>(v);
+#pragma unroll
+  for (int r = 0; r < 16; ++r) s[pad(row * L + t * 16 + r)] = v[out_slot<16>(r)];
+}
+
+// Inverse last stage (radix 16, NS = L/16): leaves X[t + r*TR] in o[r].
+template <int L, int TR>
+__device__ __forceinline__ void last_stage_to_regs(const double2 *s, const double2 *__restrict__ tw, double2 *o,
+                                                   int row, int t) {
+  double2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = s[pad(row * L + t + r * TR)];
+#pragma unroll
+  for (int r = 1; r < 16; ++r) v[r] = cmulc(v[r], __ldg(&tw[r * t]));
+  dft<16, -1>(v);
+#pragma unroll
+  for (int r = 0; r < 16; ++r) o[r] = v[out_slot<16>(r)];
+}
+
+template <class P>
+constexpr int tall_threads() { return 2 * (P::L / 16); }
+
+// Blocks per SM to ask of the register allocator: about 128 registers per
+// thread, which leaves room for two or more CTAs per SM.
+constexpr int min_blocks(int threads) { return 65536 / (threads * 128) > 1 ? 65536 / (threads * 128) : 1; }
+
+// Tall pass for columns of length H = P::L; two columns per CTA.
+template <class P>
+__global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>())) tall_static(TallArgs a) {
+  constexpr int H = P::L, TR = H / 16;
+  static_assert(P::a[0] == 16, "first radix must be 16");
+  extern __shared__ double2 sm[];
+  const int c = blockIdx.x;
+  const int W = a.W;
+  const bool special = (c == 0);
+  const int kA = special ? 0 : c;
+  const int kB = special ? W / 2 : W - c;
+  const int col = threadIdx.x / TR, t = threadIdx.x - col * TR;
+  const int k1 = col ? kB : kA;
+  if (c == 0 && threadIdx.x == 0) {
+    const uint32_t o = a.st->offset;  // CUDALucas.cu:1882, once per iteration
+    a.st->offset = (uint32_t)((2ull * o) % a.q);
+  }
+  const double2 *src = a.A + (size_t)k1 * H;
+  {
+    double2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m2 = t + r * TR;
+      v[r] = cmul(src[m2], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
+    }
+    first_stage_from_regs<H, TR>(sm, v, col, t);
+  }
+  __syncthreads();
+  fwd_stages<P, 1, P::N, 16, TR>(sm, a.twH, col, t);
+  if (!special) {
+    for (int k2 = threadIdx.x; k2 < H; k2 += 2 * TR) {
+      double2 za = sm[pad(k2)], zb = sm[pad(2 * H - 1 - k2)];
+      pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, kA + W * k2));
+      sm[pad(k2)] = za;
+      sm[pad(2 * H - 1 - k2)] = zb;
+    }
+  } else {
+    const int half = H / 2;
+    for (int i = threadIdx.x; i <= half; i += 2 * TR) {
+      const int p = (H - i) % H;
+      double2 za = sm[pad(i)], zb = sm[pad(p)];
+      pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W * i));
+      sm[pad(i)] = za;
+      if (p != i) sm[pad(p)] = zb;
+    }
+    for (int i = threadIdx.x; i < half; i += 2 * TR) {
+      double2 za = sm[pad(H + i)], zb = sm[pad(2 * H - 1 - i)];
+      pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W / 2 + W * i));
+      sm[pad(H + i)] = za;
+      sm[pad(2 * H - 1 - i)] = zb;
+    }
+  }
+  __syncthreads();
+  inv_stages<P, 0, P::N - 1, 1, TR>(sm, a.twH, col, t);
+  double2 o[16];
+  last_stage_to_regs<H, TR>(sm, a.twH, o, col, t);
+  double2 *dst = a.A + (size_t)k1 * H;
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const int m2 = t + r * TR;
+    dst[m2] = cmulc(o[r], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
+  }
+}
+
+template <class P, int G>
+constexpr int wide_threads() { return G * (P::L / 16); }
+
+// Wide pass for rows of length W = P::L; G rows per CTA.
+template <class P, int G, int MODE>
+__global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<P, G>())) wide_static(WideArgs a) {
+  constexpr int W = P::L, TR = W / 16, T = G * TR;
+  static_assert(P::a[0] == 16, "first radix must be 16");
+  extern __shared__ double2 sm[];
+  __shared__ int s_g;
+  __shared__ float s_err[32];
+  __shared__ uint32_t s_fault;
+  if (threadIdx.x == 0) {
+    s_fault = 0;
+    s_g = MODE == WIDE_INIT ? (int)blockIdx.x
+                            : (int)(atomicAdd(&a.st->ticket, 1ull) % (unsigned long long)a.ngroups);
+  }
+  __syncthreads();
+  const int g = s_g;
+  const int H = a.H;
+  const int m2b = g * G;
+  const int row = threadIdx.x / TR, t = threadIdx.x - row * TR;
+  const int m2 = m2b + row;
+  const int n = (int)a.n, bb = (int)a.b, qn = (int)a.qn;
+  // per-row weight constants of words 2*m2 and 2*m2+1
+  const int eR0 = __ldg(&a.rowE[2 * m2]), eR1 = __ldg(&a.rowE[2 * m2 + 1]);
+  const double rw0 = __ldg(&a.rowW[2 * m2]), rw1 = __ldg(&a.rowW[2 * m2 + 1]);
+  double2 x[16];
+  float emax = 0.f;
+  uint32_t fault = 0;
+
+  if (MODE != WIDE_INIT) {
+    for (int idx = threadIdx.x; idx < G * W; idx += T) {
+      const int k1 = idx / G, r = idx - k1 * G;
+      sm[pad(r * W + k1)] = a.A[(size_t)k1 * H + m2b + r];
+    }
+    __syncthreads();
+    inv_stages<P, 0, P::N - 1, 1, TR>(sm, a.twW, row, t);
+    double2 u[16];
+    last_stage_to_regs<W, TR>(sm, a.twW, u, row, t);
+    __syncthreads();  // shared memory is reused for the carry hand-off below
+
+    const double rwi0 = __ldg(&a.rowWi[2 * m2]), rwi1 = __ldg(&a.rowWi[2 * m2 + 1]);
+    const uint32_t off = a.st->offset;
+    const uint32_t pos = (off + 1) % a.q;
+    const uint32_t dw = (uint32_t)(((unsigned long long)pos * a.n) / a.q);
+    const uint32_t sdw = (uint32_t)(((unsigned long long)dw * a.q + a.n - 1) / a.n);
+    const long long sub = 1ll << (pos - sdw);
+    long long *cs = reinterpret_cast<long long *>(sm);
+    long long v0[16], v1[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m1 = t + r * TR;
+      const int f = __ldg(&a.colF[m1]);
+      const double cwi = __ldg(&a.colWi[m1]);
+      const int e0 = eR0 + f, e1 = eR1 + f;
+      const bool w0 = e0 >= n, w1 = e1 >= n;
+      const double t0 = u[r].x * (rwi0 * cwi * (w0 ? 2.0 : 1.0));
+      const double t1 = u[r].y * (rwi1 * cwi * (w1 ? 2.0 : 1.0));
+      const double r0 = rint(t0), r1 = rint(t1);
+      emax = fmaxf(emax, fmaxf(fabsf((float)(t0 - r0)), fabsf((float)(t1 - r1))));
+      long long a0 = (long long)r0, a1 = (long long)r1;
+      const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
+      if (j0 == dw) a0 -= sub;
+      if (j0 + 1 == dw) a1 -= sub;
+      v0[r] = a0;
+      v1[r] = a1;
+      const int b0 = qn + ((w0 ? e0 - n : e0) < bb ? 1 : 0);
+      const int b1 = qn + ((w1 ? e1 - n : e1) < bb ? 1 : 0);
+      const long long pc = element_carry(a0, a1, b0, b1, fault);
+      cs[row * W + m1] = pc;
+      if (row == G - 1) a.carry[(size_t)g * W + m1] = pc;
+    }
+    __threadfence();
+    __syncthreads();
+    const int pred = g == 0 ? a.ngroups - 1 : g - 1;
+    if (threadIdx.x == 0) {
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&a.flags[g]), "r"(1u) : "memory");
+      if (!wait_flag(&a.flags[pred])) s_fault |= 1u;
+      a.flags[pred] = 0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m1 = t + r * TR;
+      long long cin;
+      if (row > 0) cin = cs[(row - 1) * W + m1];
+      else cin = __ldcg(&a.carry[(size_t)pred * W + (g == 0 ? (m1 == 0 ? W - 1 : m1 - 1) : m1)]);
+      const int f = __ldg(&a.colF[m1]);
+      const double cw = __ldg(&a.colW[m1]);
+      const int e0 = eR0 + f, e1 = eR1 + f;
+      const bool w0 = e0 >= n, w1 = e1 >= n;
+      const int b0 = qn + ((w0 ? e0 - n : e0) < bb ? 1 : 0);
+      const int b1 = qn + ((w1 ? e1 - n : e1) < bb ? 1 : 0);
+      long long C1, C2;
+      unpack_carry(cin, C1, C2);
+      const long long low0 = v0[r] & ((1ll << b0) - 1), h0 = v0[r] >> b0;
+      const long long low1 = v1[r] & ((1ll << b1) - 1);
+      const long long tt1 = low1 + h0;
+      const long long k1c = (tt1 + (1ll << (b1 - 1))) >> b1;
+      const long long d1p = tt1 - (k1c << b1);
+      const long long tt0 = low0 + C1;
+      const long long k0 = (tt0 + (1ll << (b0 - 1))) >> b0;
+      const long long d0p = tt0 - (k0 << b0);
+      const long long d0 = d0p + C2, d1 = d1p + k0;
+      if (MODE == WIDE_REPORT) {
+        const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
+        a.xint[j0] = (int32_t)d0;
+        a.xint[j0 + 1] = (int32_t)d1;
+      }
+      x[r] = make_double2((double)d0 * (rw0 * cw * (w0 ? 0.5 : 1.0)), (double)d1 * (rw1 * cw * (w1 ? 0.5 : 1.0)));
+    }
+    __syncthreads();  // carry reads done before the data region is rewritten
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m1 = t + r * TR;
+      const int f = __ldg(&a.colF[m1]);
+      const double cw = __ldg(&a.colW[m1]);
+      const int e0 = eR0 + f, e1 = eR1 + f;
+      const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
+      x[r] = make_double2((double)a.xint[j0] * (rw0 * cw * (e0 >= n ? 0.5 : 1.0)),
+                          (double)a.xint[j0 + 1] * (rw1 * cw * (e1 >= n ? 0.5 : 1.0)));
+    }
+  }
+  first_stage_from_regs<W, TR>(sm, x, row, t);
+  __syncthreads();
+  fwd_stages<P, 1, P::N, 16, TR>(sm, a.twW, row, t);
+  for (int idx = threadIdx.x; idx < G * W; idx += T) {
+    const int k1 = idx / G, r = idx - k1 * G;
+    a.A[(size_t)k1 * H + m2b + r] = sm[pad(r * W + k1)];
+  }
+  if (MODE != WIDE_INIT) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+    if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = emax;
+    if (fault) atomicOr(&s_fault, fault);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float m = 0.f;
+      for (int i = 0; i < (T + 31) / 32; ++i) m = fmaxf(m, s_err[i]);
+      atomicMax(&a.st->err_bits, __float_as_uint(m));
+      if (s_fault) atomicOr(&a.st->fault, s_fault);
+    }
+  }
+}

@@ -10,7 +10,7 @@ import pytest
 
 import cudalucas_b200 as cl
 import ibdwt_model
-from golden_data import kats, large_entries
+from golden_data import kats, large_entries, reference_run_entries
 from oracle import exact
 from oracle.binding import Oracle
 
@@ -117,22 +117,22 @@ def test_c1_full_test_216091_is_prime():
         assert maxerr < 0.4
 
 
-def test_c2_3200k_kat_at_10000():
+def test_c2_3200k_matches_exact_kat_and_reference_binary():
     q, n = 57885161, 3276800
-    checks = {k: r for p, k, r in large_entries() if p == q}
+    checks = {k: r for p, k, r in large_entries() + reference_run_entries() if p == q}
     with cl.LLContext(q, n) as c:
         c.start(0)
         done = 0
-        for k in sorted(list(checks) + [10000]):
+        for k in sorted(set(checks) | {10000}):
             err = c.step(k - done, report=True)
             done = k
             assert err < 0.4
-            assert c.res64() == (KAT[q] if k == 10000 else checks[k])
+            assert c.res64() == checks.get(k, KAT[q] if k == 10000 else None)
 
 
-def test_c3_18432k_matches_exact():
+def test_c3_18432k_matches_exact_and_reference_binary():
     q, n = 332192831, 18874368
-    checks = {k: r for p, k, r in large_entries() if p == q}
+    checks = {k: r for p, k, r in large_entries() + reference_run_entries() if p == q}
     if not checks:
         pytest.skip("large fixture not generated")
     with cl.LLContext(q, n) as c:
