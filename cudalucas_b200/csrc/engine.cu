@@ -55,6 +55,7 @@ struct DevState {
 
 struct TallArgs {
   double2 *A;
+  const double2 *stw;   // stage twiddles of the specialised column transform
   const double2 *twH;   // e^{2 pi i e/H}
   const double2 *thi;   // e^{2 pi i (e<<TS)/N}
   const double2 *tlo;   // e^{2 pi i e/N}, e < 2^TS
@@ -66,6 +67,7 @@ struct TallArgs {
 
 struct WideArgs {
   double2 *A;
+  const double2 *stw;   // stage twiddles of the specialised row transform
   int32_t *xint;
   long long *carry;     // packed carries, one row of W per CTA
   uint32_t *flags;      // one ready flag per CTA
@@ -354,15 +356,21 @@ struct StaticWide {
   void (*iter)(WideArgs);
   void (*report)(WideArgs);
   void (*init)(WideArgs);
+  int nrad, rad[4];
+  int extra;  // shared-memory entries beyond the rows (stage twiddles)
 };
 struct StaticTall {
   int L;
   void (*run)(TallArgs);
+  int nrad, rad[4];
+  int extra;
 };
 
-#define LLB_WIDE(LIST, G) \
-  {LIST::L, G, wide_static<LIST, G, WIDE_ITER>, wide_static<LIST, G, WIDE_REPORT>, wide_static<LIST, G, WIDE_INIT>}
-#define LLB_TALL(LIST) {LIST::L, tall_static<LIST>}
+#define LLB_WIDE(LIST, G)                                                                                       \
+  {LIST::L, G, wide_static<LIST, G, WIDE_ITER>, wide_static<LIST, G, WIDE_REPORT>, wide_static<LIST, G, WIDE_INIT>, \
+   LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tw_size<LIST>()}
+#define LLB_TALL(LIST) \
+  {LIST::L, tall_static<LIST>, LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tall_extra<LIST>()}
 
 using L512 = RList<16, 2, 16>;
 using L768 = RList<16, 3, 16>;
@@ -551,6 +559,28 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
   return false;
 }
 
+size_t shape_wide_smem(const Shape &s) {
+  return wide_smem(s.W, s.G) + (s.sw ? sizeof(double2) * (size_t)s.sw->extra : 0);
+}
+size_t shape_tall_smem(const Shape &s) {
+  return tall_smem(s.H) + (s.st ? sizeof(double2) * (size_t)s.st->extra : 0);
+}
+
+// Stage twiddles of a radix list in the order the specialised kernels read
+// them: for each stage with NS > 1, rows k < NS of w_{NS*R}^(r*k), r = 1..R-1.
+std::vector<double2> stage_twiddles(const int *rad, int nrad) {
+  std::vector<double2> out;
+  long long ns = 1;
+  for (int i = 0; i < nrad; ++i) {
+    const int R = rad[i];
+    if (ns > 1)
+      for (long long k = 0; k < ns; ++k)
+        for (int r = 1; r < R; ++r) out.push_back(unit_root((unsigned long long)(r * k), (unsigned long long)(ns * R)));
+    ns *= R;
+  }
+  return out;
+}
+
 }  // namespace
 
 struct ll_ctx {
@@ -568,6 +598,7 @@ struct ll_ctx {
   uint32_t *flags = nullptr;
   DevState *st = nullptr;
   double2 *twW = nullptr, *twH = nullptr, *thi = nullptr, *tlo = nullptr;
+  double2 *stwW = nullptr, *stwH = nullptr;
   int32_t *rowE = nullptr, *colF = nullptr;
   double *rowW = nullptr, *rowWi = nullptr, *colW = nullptr, *colWi = nullptr;
   // host mirror
@@ -606,7 +637,7 @@ static void free_ctx(ll_ctx *c) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
-  void *ptrs[] = {c->A, c->xint, c->carry, c->flags, c->st, c->twW, c->twH, c->thi, c->tlo,
+  void *ptrs[] = {c->A, c->xint, c->carry, c->flags, c->st, c->twW, c->twH, c->thi, c->tlo, c->stwW, c->stwH,
                   c->rowE, c->colF, c->rowW, c->rowWi, c->colW, c->colWi};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -649,6 +680,16 @@ static ll_status build_tables(ll_ctx *ctx) {
     cF[m1] = (int32_t)e;
     cW[m1] = (double)exp2l((long double)e / LN);
     cWi[m1] = (double)exp2l(-(long double)e / LN);
+  }
+  if (ctx->shape.sw) {
+    std::vector<double2> t = stage_twiddles(ctx->shape.sw->rad, ctx->shape.sw->nrad);
+    if ((int)t.size() != ctx->shape.sw->extra) return LL_ERR_SHAPE;
+    CK(upload(&ctx->stwW, t));
+  }
+  if (ctx->shape.st) {
+    std::vector<double2> t = stage_twiddles(ctx->shape.st->rad, ctx->shape.st->nrad);
+    if ((int)t.size() + 40 != ctx->shape.st->extra) return LL_ERR_SHAPE;
+    CK(upload(&ctx->stwH, t));
   }
   CK(upload(&ctx->rowE, rE));
   CK(upload(&ctx->rowW, rW));
@@ -722,7 +763,7 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
       static std::mutex mu;
       static size_t max_sw = 0, max_st = 0;
       std::lock_guard<std::mutex> lock(mu);
-      const size_t sw = std::max(max_sw, wide_smem(s.W, s.G)), st = std::max(max_st, tall_smem(s.H));
+      const size_t sw = std::max(max_sw, shape_wide_smem(s)), st = std::max(max_st, shape_tall_smem(s));
       if ((e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_ITER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
           (e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_REPORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
           (e = cudaFuncSetAttribute(wide_kernel<EPT, WIDE_INIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
@@ -747,10 +788,10 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
       max_st = st;
     }
     TallArgs &ta = ctx->ta;
-    ta.A = ctx->A; ta.twH = ctx->twH; ta.thi = ctx->thi; ta.tlo = ctx->tlo; ta.st = ctx->st;
+    ta.A = ctx->A; ta.stw = ctx->stwH; ta.twH = ctx->twH; ta.thi = ctx->thi; ta.tlo = ctx->tlo; ta.st = ctx->st;
     ta.ph = ctx->ph; ta.W = s.W; ta.H = s.H; ta.N = ctx->N; ta.ts = ctx->ts; ta.tmask = (1 << ctx->ts) - 1; ta.q = q;
     WideArgs &wa = ctx->wa;
-    wa.A = ctx->A; wa.xint = ctx->xint; wa.carry = ctx->carry; wa.flags = ctx->flags; wa.twW = ctx->twW;
+    wa.A = ctx->A; wa.stw = ctx->stwW; wa.xint = ctx->xint; wa.carry = ctx->carry; wa.flags = ctx->flags; wa.twW = ctx->twW;
     wa.rowE = ctx->rowE; wa.rowW = ctx->rowW; wa.rowWi = ctx->rowWi;
     wa.colF = ctx->colF; wa.colW = ctx->colW; wa.colWi = ctx->colWi;
     wa.st = ctx->st; wa.pw = ctx->pw; wa.W = s.W; wa.H = s.H; wa.G = s.G; wa.ngroups = ngroups;
@@ -769,7 +810,7 @@ void ll_destroy(ll_ctx *ctx) { free_ctx(ctx); }
 
 static void launch_wide(ll_ctx *ctx, int mode) {
   const Shape &s = ctx->shape;
-  const size_t sm = wide_smem(s.W, s.G);
+  const size_t sm = shape_wide_smem(s);
   if (s.sw) {
     void (*k)(WideArgs) = mode == WIDE_INIT ? s.sw->init : mode == WIDE_REPORT ? s.sw->report : s.sw->iter;
     k<<<s.H / s.G, s.T1, sm, ctx->stream>>>(ctx->wa);
@@ -784,7 +825,7 @@ static void launch_wide(ll_ctx *ctx, int mode) {
 
 static void launch_tall(ll_ctx *ctx) {
   const Shape &s = ctx->shape;
-  if (s.st) s.st->run<<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
+  if (s.st) s.st->run<<<s.W / 2, s.T2, shape_tall_smem(s), ctx->stream>>>(ctx->ta);
   else tall_kernel<EPT><<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
 }
 

@@ -71,14 +71,38 @@ __device__ __forceinline__ constexpr int sslot(int r) {
   else return out_slot<R>(r);
 }
 
+// Stage twiddles live in one table per row length, in stage order: for
+// every stage s with NS_s > 1 (radices of the list a[] applied in order,
+// NS_s = a[0]*...*a[s-1]) the entries w_{NS_s*R_s}^(r*k) for k < NS_s,
+// r = 1..R_s-1, row k contiguous.  The lists used are palindromic, so the
+// reversed (inverse) order has the same stages and uses the same table.
+template <class P, int I>
+__host__ __device__ constexpr int tw_offset() {
+  int off = 0, ns = 1;
+  for (int i = 0; i < I; ++i) {
+    if (ns > 1) off += ns * (P::a[i] - 1);
+    ns *= P::a[i];
+  }
+  return off;
+}
+template <class P>
+__host__ __device__ constexpr int tw_size() { return tw_offset<P, P::N>(); }
+
+template <class P>
+__host__ __device__ constexpr bool palindromic() {
+  for (int i = 0; i < P::N; ++i)
+    if (P::a[i] != P::a[P::N - 1 - i]) return false;
+  return true;
+}
+
 // One Stockham stage of every row of the CTA, in place in shared memory.
 // Thread t of a row handles butterflies t, t+TR, ... (a guard skips the
-// tail when L/R is not a multiple of TR).
+// tail when L/R is not a multiple of TR).  `tw` points at this stage's
+// twiddle block (NS rows of R-1 entries) in shared memory.
 template <int L, int R, int NS, int SIGN, int TR>
-__device__ __forceinline__ void sstage(double2 *s, const double2 *__restrict__ tw, int row, int t) {
+__device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, int t) {
   constexpr int M = L / R;
   constexpr int NB = (M + TR - 1) / TR;
-  constexpr int STEP = L / (NS * R);
   double2 v[NB][R];
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
@@ -90,7 +114,7 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *__restrict__ t
         const int k = j % NS;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          const double2 w = __ldg(&tw[r * k * STEP]);
+          const double2 w = tw[k * (R - 1) + r - 1];
           v[b][r] = SIGN > 0 ? cmul(v[b][r], w) : cmulc(v[b][r], w);
         }
       }
@@ -113,20 +137,21 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *__restrict__ t
 
 // forward stages [I, E) (radix a[I], NS = a[0]*...*a[I-1])
 template <class P, int I, int E, int NS, int TR>
-__device__ __forceinline__ void fwd_stages(double2 *s, const double2 *__restrict__ tw, int row, int t) {
+__device__ __forceinline__ void fwd_stages(double2 *s, const double2 *tw, int row, int t) {
   if constexpr (I < E) {
     constexpr int R = P::a[I];
-    sstage<P::L, R, NS, +1, TR>(s, tw, row, t);
+    sstage<P::L, R, NS, +1, TR>(s, tw + tw_offset<P, I>(), row, t);
     fwd_stages<P, I + 1, E, NS * R, TR>(s, tw, row, t);
   }
 }
 
 // inverse stages [I, E) of the reversed list (radix a[N-1-I])
 template <class P, int I, int E, int NS, int TR>
-__device__ __forceinline__ void inv_stages(double2 *s, const double2 *__restrict__ tw, int row, int t) {
+__device__ __forceinline__ void inv_stages(double2 *s, const double2 *tw, int row, int t) {
+  static_assert(palindromic<P>(), "inverse stages reuse the forward twiddle table");
   if constexpr (I < E) {
     constexpr int R = P::a[P::N - 1 - I];
-    sstage<P::L, R, NS, -1, TR>(s, tw, row, t);
+    sstage<P::L, R, NS, -1, TR>(s, tw + tw_offset<P, I>(), row, t);
     inv_stages<P, I + 1, E, NS * R, TR>(s, tw, row, t);
   }
 }
@@ -140,14 +165,14 @@ __device__ __forceinline__ void first_stage_from_regs(double2 *s, double2 *v, in
 }
 
 // Inverse last stage (radix 16, NS = L/16): leaves X[t + r*TR] in o[r].
+// tw is the stage's twiddle block (k = t, 15 entries per k).
 template <int L, int TR>
-__device__ __forceinline__ void last_stage_to_regs(const double2 *s, const double2 *__restrict__ tw, double2 *o,
-                                                   int row, int t) {
+__device__ __forceinline__ void last_stage_to_regs(const double2 *s, const double2 *tw, double2 *o, int row, int t) {
   double2 v[16];
 #pragma unroll
   for (int r = 0; r < 16; ++r) v[r] = s[pad(row * L + t + r * TR)];
 #pragma unroll
-  for (int r = 1; r < 16; ++r) v[r] = cmulc(v[r], __ldg(&tw[r * t]));
+  for (int r = 1; r < 16; ++r) v[r] = cmulc(v[r], tw[t * 15 + r - 1]);
   dft<16, -1>(v);
 #pragma unroll
   for (int r = 0; r < 16; ++r) o[r] = v[out_slot<16>(r)];
@@ -160,12 +185,24 @@ constexpr int tall_threads() { return 2 * (P::L / 16); }
 // thread, which leaves room for two or more CTAs per SM.
 constexpr int min_blocks(int threads) { return 65536 / (threads * 128) > 1 ? 65536 / (threads * 128) : 1; }
 
+// Shared memory of the tall pass beyond the two columns: stage twiddles,
+// the column twiddle factors w_N^(k*TR*r) of both columns (2 x 16) and the
+// pairing-loop factors w_H^(j*2*TR) (8 entries).
+template <class P>
+__host__ __device__ constexpr int tall_extra() { return tw_size<P>() + 32 + 8; }
+
 // Tall pass for columns of length H = P::L; two columns per CTA.
+// The column twiddle w_N^(k1*m2) of element m2 = t + r*TR is formed as
+// w_N^(k1*t) (one table product per thread) times w_N^(k1*TR*r) (shared by
+// the CTA), so no per-element table gathers are needed.
 template <class P>
 __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>())) tall_static(TallArgs a) {
-  constexpr int H = P::L, TR = H / 16;
+  constexpr int H = P::L, TR = H / 16, T = 2 * TR;
   static_assert(P::a[0] == 16, "first radix must be 16");
   extern __shared__ double2 sm[];
+  double2 *stw = sm + padded(2 * H);
+  double2 *wr = stw + tw_size<P>();
+  double2 *pj = wr + 32;
   const int c = blockIdx.x;
   const int W = a.W;
   const bool special = (c == 0);
@@ -177,51 +214,70 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
     const uint32_t o = a.st->offset;  // CUDALucas.cu:1882, once per iteration
     a.st->offset = (uint32_t)((2ull * o) % a.q);
   }
+  for (int i = threadIdx.x; i < tw_size<P>(); i += T) stw[i] = a.stw[i];
+  if (threadIdx.x < 32) {
+    const int kk = threadIdx.x < 16 ? kA : kB, r = threadIdx.x & 15;
+    wr[threadIdx.x] = omegaN(a.thi, a.tlo, a.ts, a.tmask, kk * TR * r);
+  } else if (threadIdx.x < 40) {
+    pj[threadIdx.x - 32] = __ldg(&a.twH[(threadIdx.x - 32) * T]);
+  }
+  const double2 base = omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * t);
+  __syncthreads();
   const double2 *src = a.A + (size_t)k1 * H;
   {
     double2 v[16];
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int m2 = t + r * TR;
-      v[r] = cmul(src[m2], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
-    }
+    for (int r = 0; r < 16; ++r) v[r] = cmul(src[t + r * TR], cmul(base, wr[col * 16 + r]));
     first_stage_from_regs<H, TR>(sm, v, col, t);
   }
   __syncthreads();
-  fwd_stages<P, 1, P::N, 16, TR>(sm, a.twH, col, t);
+  fwd_stages<P, 1, P::N, 16, TR>(sm, stw, col, t);
+  // pairing: loop index i = threadIdx.x + j*T, w_H^i = w_H^threadIdx.x * pj[j]
+  const double2 wt = __ldg(&a.twH[threadIdx.x]);
   if (!special) {
-    for (int k2 = threadIdx.x; k2 < H; k2 += 2 * TR) {
+    const double2 wb = cmul(omegaN(a.thi, a.tlo, a.ts, a.tmask, kA), wt);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int k2 = threadIdx.x + j * T;
       double2 za = sm[pad(k2)], zb = sm[pad(2 * H - 1 - k2)];
-      pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, kA + W * k2));
+      pair_square(za, zb, cmul(wb, pj[j]));
       sm[pad(k2)] = za;
       sm[pad(2 * H - 1 - k2)] = zb;
     }
   } else {
     const int half = H / 2;
-    for (int i = threadIdx.x; i <= half; i += 2 * TR) {
-      const int p = (H - i) % H;
-      double2 za = sm[pad(i)], zb = sm[pad(p)];
-      pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W * i));
-      sm[pad(i)] = za;
-      if (p != i) sm[pad(p)] = zb;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {  // column 0: k2 <-> (H-k2) mod H, w_N^(W*k2) = w_H^k2
+      const int i = threadIdx.x + j * T;
+      if (i <= half) {
+        const int p = (H - i) % H;
+        double2 za = sm[pad(i)], zb = sm[pad(p)];
+        pair_square(za, zb, cmul(wt, pj[j]));
+        sm[pad(i)] = za;
+        if (p != i) sm[pad(p)] = zb;
+      }
     }
-    for (int i = threadIdx.x; i < half; i += 2 * TR) {
-      double2 za = sm[pad(H + i)], zb = sm[pad(2 * H - 1 - i)];
-      pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W / 2 + W * i));
-      sm[pad(H + i)] = za;
-      sm[pad(2 * H - 1 - i)] = zb;
+    if (threadIdx.x == 0) {  // i = half + ... covered above only when half < 8*T
+    }
+    const double2 wb = cmul(omegaN(a.thi, a.tlo, a.ts, a.tmask, W / 2), wt);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {  // column W/2: k2 <-> H-1-k2
+      const int i = threadIdx.x + j * T;
+      if (i < half) {
+        double2 za = sm[pad(H + i)], zb = sm[pad(2 * H - 1 - i)];
+        pair_square(za, zb, cmul(wb, pj[j]));
+        sm[pad(H + i)] = za;
+        sm[pad(2 * H - 1 - i)] = zb;
+      }
     }
   }
   __syncthreads();
-  inv_stages<P, 0, P::N - 1, 1, TR>(sm, a.twH, col, t);
+  inv_stages<P, 0, P::N - 1, 1, TR>(sm, stw, col, t);
   double2 o[16];
-  last_stage_to_regs<H, TR>(sm, a.twH, o, col, t);
+  last_stage_to_regs<H, TR>(sm, stw + tw_offset<P, P::N - 1>(), o, col, t);
   double2 *dst = a.A + (size_t)k1 * H;
 #pragma unroll
-  for (int r = 0; r < 16; ++r) {
-    const int m2 = t + r * TR;
-    dst[m2] = cmulc(o[r], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
-  }
+  for (int r = 0; r < 16; ++r) dst[t + r * TR] = cmulc(o[r], cmul(base, wr[col * 16 + r]));
 }
 
 template <class P, int G>
@@ -233,6 +289,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   constexpr int W = P::L, TR = W / 16, T = G * TR;
   static_assert(P::a[0] == 16, "first radix must be 16");
   extern __shared__ double2 sm[];
+  double2 *stw = sm + padded(G * W);
   __shared__ int s_g;
   __shared__ float s_err[32];
   __shared__ uint32_t s_fault;
@@ -241,6 +298,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
     s_g = MODE == WIDE_INIT ? (int)blockIdx.x
                             : (int)(atomicAdd(&a.st->ticket, 1ull) % (unsigned long long)a.ngroups);
   }
+  for (int i = threadIdx.x; i < tw_size<P>(); i += T) stw[i] = a.stw[i];
   __syncthreads();
   const int g = s_g;
   const int H = a.H;
@@ -261,9 +319,9 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
       sm[pad(r * W + k1)] = a.A[(size_t)k1 * H + m2b + r];
     }
     __syncthreads();
-    inv_stages<P, 0, P::N - 1, 1, TR>(sm, a.twW, row, t);
+    inv_stages<P, 0, P::N - 1, 1, TR>(sm, stw, row, t);
     double2 u[16];
-    last_stage_to_regs<W, TR>(sm, a.twW, u, row, t);
+    last_stage_to_regs<W, TR>(sm, stw + tw_offset<P, P::N - 1>(), u, row, t);
     __syncthreads();  // shared memory is reused for the carry hand-off below
 
     const double rwi0 = __ldg(&a.rowWi[2 * m2]), rwi1 = __ldg(&a.rowWi[2 * m2 + 1]);
@@ -351,7 +409,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   }
   first_stage_from_regs<W, TR>(sm, x, row, t);
   __syncthreads();
-  fwd_stages<P, 1, P::N, 16, TR>(sm, a.twW, row, t);
+  fwd_stages<P, 1, P::N, 16, TR>(sm, stw, row, t);
   for (int idx = threadIdx.x; idx < G * W; idx += T) {
     const int k1 = idx / G, r = idx - k1 * G;
     a.A[(size_t)k1 * H + m2b + r] = sm[pad(r * W + k1)];
