@@ -82,6 +82,10 @@ struct WideArgs {
   FftPlan pw;
   int W, H, G, ngroups;
   uint32_t q, n, b, qn;
+  // specialised kernels: column m1 = t + r*TR has exponent colF[t] - colD[r]
+  // (mod n), i.e. weight colW[t] * colS[r] (times 2 when it wraps)
+  int colD[16];
+  double colS[16], colSi[16];
 };
 
 __device__ __forceinline__ double2 omegaN(const double2 *__restrict__ thi, const double2 *__restrict__ tlo,
@@ -796,6 +800,16 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
     wa.colF = ctx->colF; wa.colW = ctx->colW; wa.colWi = ctx->colWi;
     wa.st = ctx->st; wa.pw = ctx->pw; wa.W = s.W; wa.H = s.H; wa.G = s.G; wa.ngroups = ngroups;
     wa.q = q; wa.n = n; wa.b = ctx->b; wa.qn = ctx->qn;
+    if (s.sw) {
+      // column m1 = t + r*TR: exponent colF[t] - D_r (mod n), D_r = r*TR*2H*b mod n
+      const long long TR = s.W / 16;
+      for (int r = 0; r < 16; ++r) {
+        const long long D = (long long)((unsigned __int128)r * TR * 2 * s.H % n * ctx->b % n);
+        wa.colD[r] = (int)D;
+        wa.colS[r] = (double)exp2l(-(long double)D / (long double)n);
+        wa.colSi[r] = (double)exp2l((long double)D / (long double)n);
+      }
+    }
   } while (0);
   cudaSetDevice(prev);
   if (rc != LL_OK) {

@@ -283,7 +283,26 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
 template <class P, int G>
 constexpr int wide_threads() { return G * (P::L / 16); }
 
+// 16-byte asynchronous global -> shared copy (no register staging).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
+// Splits an integer-valued double v (|v| < 2^52) as v = h*2^b + l, 0 <= l < 2^b
+// (exact: scaling by powers of two and floor are exact in FP64).
+__device__ __forceinline__ void split_word(double v, double p2b, double ip2b, double &h, double &l) {
+  h = floor(v * ip2b);
+  l = fma(-h, p2b, v);
+}
+
 // Wide pass for rows of length W = P::L; G rows per CTA.
+// The carry arithmetic runs in FP64 on integer-valued doubles (all values
+// stay below 2^53, so every step is exact); carries are handed over as
+// int32 pairs (c1, c2).
 template <class P, int G, int MODE>
 __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<P, G>())) wide_static(WideArgs a) {
   constexpr int W = P::L, TR = W / 16, T = G * TR;
@@ -298,62 +317,80 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
     s_g = MODE == WIDE_INIT ? (int)blockIdx.x
                             : (int)(atomicAdd(&a.st->ticket, 1ull) % (unsigned long long)a.ngroups);
   }
-  for (int i = threadIdx.x; i < tw_size<P>(); i += T) stw[i] = a.stw[i];
+  for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
   __syncthreads();
   const int g = s_g;
   const int H = a.H;
   const int m2b = g * G;
+  if (MODE != WIDE_INIT)
+    for (int idx = threadIdx.x; idx < G * W; idx += T) {
+      const int k1 = idx / G, r = idx - k1 * G;
+      cp_async16(&sm[pad(r * W + k1)], &a.A[(size_t)k1 * H + m2b + r]);
+    }
   const int row = threadIdx.x / TR, t = threadIdx.x - row * TR;
   const int m2 = m2b + row;
   const int n = (int)a.n, bb = (int)a.b, qn = (int)a.qn;
-  // per-row weight constants of words 2*m2 and 2*m2+1
+  // per-row and per-thread weight bases (word 2*m2+s, column t)
   const int eR0 = __ldg(&a.rowE[2 * m2]), eR1 = __ldg(&a.rowE[2 * m2 + 1]);
   const double rw0 = __ldg(&a.rowW[2 * m2]), rw1 = __ldg(&a.rowW[2 * m2 + 1]);
+  const int ft = __ldg(&a.colF[t]);
+  const double cwt = __ldg(&a.colW[t]);
+  const double p2lo = (double)(1 << qn), p2hi = 2.0 * p2lo;
+  const double ip2lo = 1.0 / p2lo, ip2hi = 0.5 * ip2lo;
   double2 x[16];
   float emax = 0.f;
   uint32_t fault = 0;
 
   if (MODE != WIDE_INIT) {
-    for (int idx = threadIdx.x; idx < G * W; idx += T) {
-      const int k1 = idx / G, r = idx - k1 * G;
-      sm[pad(r * W + k1)] = a.A[(size_t)k1 * H + m2b + r];
-    }
+    const double rwi0 = __ldg(&a.rowWi[2 * m2]), rwi1 = __ldg(&a.rowWi[2 * m2 + 1]);
+    const double cwit = __ldg(&a.colWi[t]);
+    const uint32_t off = a.st->offset;
+    const uint32_t pos = (off + 1) % a.q;
+    const uint32_t dw = (uint32_t)(((unsigned long long)pos * a.n) / a.q);
+    const uint32_t sdw = (uint32_t)(((unsigned long long)dw * a.q + a.n - 1) / a.n);
+    const double sub = (double)(1u << (pos - sdw));
+    cp_async_wait_all();
     __syncthreads();
     inv_stages<P, 0, P::N - 1, 1, TR>(sm, stw, row, t);
     double2 u[16];
     last_stage_to_regs<W, TR>(sm, stw + tw_offset<P, P::N - 1>(), u, row, t);
     __syncthreads();  // shared memory is reused for the carry hand-off below
 
-    const double rwi0 = __ldg(&a.rowWi[2 * m2]), rwi1 = __ldg(&a.rowWi[2 * m2 + 1]);
-    const uint32_t off = a.st->offset;
-    const uint32_t pos = (off + 1) % a.q;
-    const uint32_t dw = (uint32_t)(((unsigned long long)pos * a.n) / a.q);
-    const uint32_t sdw = (uint32_t)(((unsigned long long)dw * a.q + a.n - 1) / a.n);
-    const long long sub = 1ll << (pos - sdw);
-    long long *cs = reinterpret_cast<long long *>(sm);
-    long long v0[16], v1[16];
+    int2 *cs = reinterpret_cast<int2 *>(sm);
+    int2 *gc = reinterpret_cast<int2 *>(a.carry);
+    // kept across the hand-off: low part of word 0 and balanced word 1
+    int2 keep[16];
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
-      const int f = __ldg(&a.colF[m1]);
-      const double cwi = __ldg(&a.colWi[m1]);
+      const int fr = ft - a.colD[r];
+      const bool fw = fr < 0;
+      const int f = fw ? fr + n : fr;
+      const double cwi = cwit * a.colSi[r] * (fw ? 0.5 : 1.0);
       const int e0 = eR0 + f, e1 = eR1 + f;
       const bool w0 = e0 >= n, w1 = e1 >= n;
       const double t0 = u[r].x * (rwi0 * cwi * (w0 ? 2.0 : 1.0));
       const double t1 = u[r].y * (rwi1 * cwi * (w1 ? 2.0 : 1.0));
-      const double r0 = rint(t0), r1 = rint(t1);
+      double r0 = rint(t0), r1 = rint(t1);
       emax = fmaxf(emax, fmaxf(fabsf((float)(t0 - r0)), fabsf((float)(t1 - r1))));
-      long long a0 = (long long)r0, a1 = (long long)r1;
       const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
-      if (j0 == dw) a0 -= sub;
-      if (j0 + 1 == dw) a1 -= sub;
-      v0[r] = a0;
-      v1[r] = a1;
-      const int b0 = qn + ((w0 ? e0 - n : e0) < bb ? 1 : 0);
-      const int b1 = qn + ((w1 ? e1 - n : e1) < bb ? 1 : 0);
-      const long long pc = element_carry(a0, a1, b0, b1, fault);
+      if (j0 == dw) r0 -= sub;
+      if (j0 + 1 == dw) r1 -= sub;
+      const bool big0 = (w0 ? e0 - n : e0) < bb, big1 = (w1 ? e1 - n : e1) < bb;
+      const double P1 = big1 ? p2hi : p2lo, I1 = big1 ? ip2hi : ip2lo;
+      // word i keeps bal(low_i + c1_{i-1}) + c2_{i-1}: c1 is the high part of
+      // the previous word, c2 the carry out of balancing the previous word
+      double h0, l0, h1, l1;
+      split_word(r0, big0 ? p2hi : p2lo, big0 ? ip2hi : ip2lo, h0, l0);
+      split_word(r1, P1, I1, h1, l1);
+      const double tt1 = l1 + h0;
+      const double k1c = floor((tt1 + 0.5 * P1) * I1);
+      const double d1p = fma(-k1c, P1, tt1);
+      if (fabs(h1) >= 2147483647.0 || fabs(k1c) >= 2147483647.0) fault |= 2u;
+      keep[r] = make_int2((int)l0, (int)d1p);
+      const int2 pc = make_int2((int)h1, (int)k1c);  // outgoing (c1, c2)
       cs[row * W + m1] = pc;
-      if (row == G - 1) a.carry[(size_t)g * W + m1] = pc;
+      if (row == G - 1) gc[(size_t)g * W + m1] = pc;
     }
     __threadfence();
     __syncthreads();
@@ -367,40 +404,42 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
-      long long cin;
+      int2 cin;
       if (row > 0) cin = cs[(row - 1) * W + m1];
-      else cin = __ldcg(&a.carry[(size_t)pred * W + (g == 0 ? (m1 == 0 ? W - 1 : m1 - 1) : m1)]);
-      const int f = __ldg(&a.colF[m1]);
-      const double cw = __ldg(&a.colW[m1]);
+      else {
+        const long long raw = __ldcg(&a.carry[(size_t)pred * W + (g == 0 ? (m1 == 0 ? W - 1 : m1 - 1) : m1)]);
+        cin = make_int2((int)(raw & 0xffffffffll), (int)(raw >> 32));
+      }
+      const int fr = ft - a.colD[r];
+      const bool fw = fr < 0;
+      const int f = fw ? fr + n : fr;
+      const double cw = cwt * a.colS[r] * (fw ? 2.0 : 1.0);
       const int e0 = eR0 + f, e1 = eR1 + f;
       const bool w0 = e0 >= n, w1 = e1 >= n;
-      const int b0 = qn + ((w0 ? e0 - n : e0) < bb ? 1 : 0);
-      const int b1 = qn + ((w1 ? e1 - n : e1) < bb ? 1 : 0);
-      long long C1, C2;
-      unpack_carry(cin, C1, C2);
-      const long long low0 = v0[r] & ((1ll << b0) - 1), h0 = v0[r] >> b0;
-      const long long low1 = v1[r] & ((1ll << b1) - 1);
-      const long long tt1 = low1 + h0;
-      const long long k1c = (tt1 + (1ll << (b1 - 1))) >> b1;
-      const long long d1p = tt1 - (k1c << b1);
-      const long long tt0 = low0 + C1;
-      const long long k0 = (tt0 + (1ll << (b0 - 1))) >> b0;
-      const long long d0p = tt0 - (k0 << b0);
-      const long long d0 = d0p + C2, d1 = d1p + k0;
+      const bool big0 = (w0 ? e0 - n : e0) < bb;
+      const double P0 = big0 ? p2hi : p2lo, I0 = big0 ? ip2hi : ip2lo;
+      const double tt0 = (double)keep[r].x + (double)cin.x;
+      const double k0 = floor((tt0 + 0.5 * P0) * I0);
+      const double d0 = fma(-k0, P0, tt0) + (double)cin.y;
+      const double d1 = (double)keep[r].y + k0;
       if (MODE == WIDE_REPORT) {
         const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
         a.xint[j0] = (int32_t)d0;
         a.xint[j0 + 1] = (int32_t)d1;
       }
-      x[r] = make_double2((double)d0 * (rw0 * cw * (w0 ? 0.5 : 1.0)), (double)d1 * (rw1 * cw * (w1 ? 0.5 : 1.0)));
+      x[r] = make_double2(d0 * (rw0 * cw * (w0 ? 0.5 : 1.0)), d1 * (rw1 * cw * (w1 ? 0.5 : 1.0)));
     }
     __syncthreads();  // carry reads done before the data region is rewritten
   } else {
+    cp_async_wait_all();
+    __syncthreads();
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
-      const int f = __ldg(&a.colF[m1]);
-      const double cw = __ldg(&a.colW[m1]);
+      const int fr = ft - a.colD[r];
+      const bool fw = fr < 0;
+      const int f = fw ? fr + n : fr;
+      const double cw = cwt * a.colS[r] * (fw ? 2.0 : 1.0);
       const int e0 = eR0 + f, e1 = eR1 + f;
       const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
       x[r] = make_double2((double)a.xint[j0] * (rw0 * cw * (e0 >= n ? 0.5 : 1.0)),
