@@ -994,3 +994,218 @@ int32_t ll_length_supported(uint32_t n) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// Some callers cannot call cudaMalloc: code running inside a memory pool or
+// arena that owns all device memory, plugins whose host forbids allocation
+// during a work call, and latency-critical loops that must not hit the
+// allocator.  ll_step_static runs the same tall/wide kernels as ll_step, but
+// every piece of device scratch -- the transform array, the carry hand-off
+// rows, the ready flags, the device state and all tables -- is carved out of
+// one file-scope __device__ array of LL_STATIC_SCRATCH_BYTES bytes.  Every GPU
+// that loads this library holds that array until the process exits.
+namespace {
+constexpr size_t kScratchBytes = LL_STATIC_SCRATCH_BYTES;
+}
+static __device__ __align__(256) unsigned char g_ll_scratch[kScratchBytes];
+
+namespace {
+
+// Host-side table staging, also file-scope so that no call allocates.
+constexpr size_t kHostTableBytes = 2u << 20;
+alignas(256) unsigned char g_host_tables[kHostTableBytes];
+std::mutex g_static_mu;
+void *g_scratch_ptr[64] = {nullptr};  // device address of g_ll_scratch, per device
+
+size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Raises (never lowers) a kernel's dynamic shared-memory limit.
+cudaError_t raise_smem_limit(const void *k, size_t bytes) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, k);
+  if (e != cudaSuccess) return e;
+  if ((size_t)fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+
+extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t offset, uint32_t iters,
+                                    const int32_t *digits_in, int32_t *digits_out, float *max_err,
+                                    void *stream) {
+  if (!digits_in || !digits_out || n < 64 || n % 4 || q <= n || (q & 1) == 0 || offset >= q) return LL_ERR_ARG;
+  if (n > LL_STATIC_MAX_WORDS) return LL_ERR_ARG;  // beyond the static scratch's stated maximum
+  if (device < 0 || device >= 64) return LL_ERR_ARG;
+  const int N = (int)(n / 2);
+  Shape s;
+  if (!choose_shape(N, nullptr, s)) return LL_ERR_SHAPE;
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (cudaSetDevice(device) != cudaSuccess) return LL_ERR_CUDA;
+  struct Restore {
+    int d;
+    ~Restore() { cudaSetDevice(d); }
+  } restore{prev};
+  cudaStream_t st = (cudaStream_t)stream;
+  // set-up, once per device: the device address of the static array
+  if (!g_scratch_ptr[device]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_ll_scratch) != cudaSuccess || !p) return LL_ERR_CUDA;
+    g_scratch_ptr[device] = p;
+  }
+  unsigned char *base = (unsigned char *)g_scratch_ptr[device];
+
+  // ---- host tables (same definitions as build_tables) into the static staging
+  const int W = s.W, H = s.H;
+  const uint32_t b = q % n, qn = q / n;
+  int ts = 0;
+  while ((1 << (ts + 1)) * (long long)(1 << (ts + 1)) <= (long long)N * 4 && ts < 14) ++ts;
+  const size_t n_lo = (size_t)1 << ts, n_hi = (size_t)(N >> ts) + 1;
+  size_t ho = 0;
+  auto hput = [&](size_t bytes) -> unsigned char * {
+    unsigned char *p = g_host_tables + ho;
+    ho = align256(ho + bytes);
+    return ho <= kHostTableBytes ? p : nullptr;
+  };
+  double2 *h_twW = (double2 *)hput(sizeof(double2) * W);
+  double2 *h_twH = (double2 *)hput(sizeof(double2) * H);
+  double2 *h_lo = (double2 *)hput(sizeof(double2) * n_lo);
+  double2 *h_hi = (double2 *)hput(sizeof(double2) * n_hi);
+  int32_t *h_rE = (int32_t *)hput(sizeof(int32_t) * 2 * H);
+  double *h_rW = (double *)hput(sizeof(double) * 2 * H);
+  double *h_rWi = (double *)hput(sizeof(double) * 2 * H);
+  int32_t *h_cF = (int32_t *)hput(sizeof(int32_t) * W);
+  double *h_cW = (double *)hput(sizeof(double) * W);
+  double *h_cWi = (double *)hput(sizeof(double) * W);
+  const size_t n_stwW = s.sw ? (size_t)s.sw->extra : 0, n_stwH = s.st ? (size_t)(s.st->extra - 40) : 0;
+  double2 *h_stwW = (double2 *)hput(sizeof(double2) * (n_stwW ? n_stwW : 1));
+  double2 *h_stwH = (double2 *)hput(sizeof(double2) * (n_stwH ? n_stwH : 1));
+  if (!h_stwH) return LL_ERR_ARG;
+  const size_t table_bytes = ho;
+  for (int e = 0; e < W; ++e) h_twW[e] = unit_root(e, W);
+  for (int e = 0; e < H; ++e) h_twH[e] = unit_root(e, H);
+  for (size_t e = 0; e < n_lo; ++e) h_lo[e] = unit_root(e, N);
+  for (size_t e = 0; e < n_hi; ++e) h_hi[e] = unit_root((unsigned long long)e << ts, N);
+  const long double LN = (long double)n;
+  for (int jr = 0; jr < 2 * H; ++jr) {
+    long long e = (-(long long)jr * b) % (long long)n;
+    if (e < 0) e += n;
+    h_rE[jr] = (int32_t)e;
+    h_rW[jr] = (double)exp2l((long double)e / LN);
+    h_rWi[jr] = (double)(exp2l(-(long double)e / LN) / (long double)N);
+  }
+  for (int m1 = 0; m1 < W; ++m1) {
+    long long e = (-((long long)2 * H * m1 % (long long)n) * (long long)b) % (long long)n;
+    if (e < 0) e += n;
+    h_cF[m1] = (int32_t)e;
+    h_cW[m1] = (double)exp2l((long double)e / LN);
+    h_cWi[m1] = (double)exp2l(-(long double)e / LN);
+  }
+  auto fill_stw = [](double2 *out, const int *rad, int nrad) {
+    size_t k = 0;
+    long long ns = 1;
+    for (int i = 0; i < nrad; ++i) {
+      const int R = rad[i];
+      if (ns > 1)
+        for (long long kk = 0; kk < ns; ++kk)
+          for (int r = 1; r < R; ++r) out[k++] = unit_root((unsigned long long)(r * kk), (unsigned long long)(ns * R));
+      ns *= R;
+    }
+    return k;
+  };
+  if (s.sw && fill_stw(h_stwW, s.sw->rad, s.sw->nrad) != n_stwW) return LL_ERR_SHAPE;
+  if (s.st && fill_stw(h_stwH, s.st->rad, s.st->nrad) != n_stwH) return LL_ERR_SHAPE;
+
+  // ---- device carve-up of the static scratch
+  const int ngroups = H / s.G;
+  size_t o = 0;
+  auto dput = [&](size_t bytes) -> unsigned char * {
+    unsigned char *p = base + o;
+    o = align256(o + bytes);
+    return p;
+  };
+  double2 *A = (double2 *)dput(sizeof(double2) * (size_t)N);
+  long long *carry = (long long *)dput(sizeof(long long) * (size_t)ngroups * W);
+  uint32_t *flags = (uint32_t *)dput(sizeof(uint32_t) * (size_t)ngroups);
+  DevState *dst = (DevState *)dput(sizeof(DevState));
+  unsigned char *dtab = dput(table_bytes);
+  if (o > kScratchBytes) return LL_ERR_ARG;  // shape needs more scratch than the static array holds
+  auto dev = [&](const void *hp) { return dtab + ((const unsigned char *)hp - g_host_tables); };
+
+  // ---- kernels' limits (raised only), arguments
+  const size_t sw_bytes = shape_wide_smem(s), st_bytes = shape_tall_smem(s);
+  cudaError_t e = cudaSuccess;
+  if (s.sw) {
+    if ((e = raise_smem_limit((const void *)s.sw->iter, sw_bytes)) != cudaSuccess ||
+        (e = raise_smem_limit((const void *)s.sw->report, sw_bytes)) != cudaSuccess ||
+        (e = raise_smem_limit((const void *)s.sw->init, sw_bytes)) != cudaSuccess)
+      return LL_ERR_CUDA;
+  } else if ((e = raise_smem_limit((const void *)wide_kernel<EPT, WIDE_ITER>, sw_bytes)) != cudaSuccess ||
+             (e = raise_smem_limit((const void *)wide_kernel<EPT, WIDE_REPORT>, sw_bytes)) != cudaSuccess ||
+             (e = raise_smem_limit((const void *)wide_kernel<EPT, WIDE_INIT>, sw_bytes)) != cudaSuccess) {
+    return LL_ERR_CUDA;
+  }
+  if ((e = raise_smem_limit(s.st ? (const void *)s.st->run : (const void *)tall_kernel<EPT>, st_bytes)) !=
+      cudaSuccess)
+    return LL_ERR_CUDA;
+  FftPlan pw, ph;
+  make_plan(W, pw);
+  make_plan(H, ph);
+  TallArgs ta{};
+  ta.A = A; ta.stw = (const double2 *)dev(h_stwH); ta.twH = (const double2 *)dev(h_twH);
+  ta.thi = (const double2 *)dev(h_hi); ta.tlo = (const double2 *)dev(h_lo); ta.st = dst;
+  ta.ph = ph; ta.W = W; ta.H = H; ta.N = N; ta.ts = ts; ta.tmask = (1 << ts) - 1; ta.q = q;
+  WideArgs wa{};
+  wa.A = A; wa.stw = (const double2 *)dev(h_stwW); wa.carry = carry; wa.flags = flags;
+  wa.twW = (const double2 *)dev(h_twW);
+  wa.rowE = (const int32_t *)dev(h_rE); wa.rowW = (const double *)dev(h_rW); wa.rowWi = (const double *)dev(h_rWi);
+  wa.colF = (const int32_t *)dev(h_cF); wa.colW = (const double *)dev(h_cW); wa.colWi = (const double *)dev(h_cWi);
+  wa.st = dst; wa.pw = pw; wa.W = W; wa.H = H; wa.G = s.G; wa.ngroups = ngroups;
+  wa.q = q; wa.n = n; wa.b = b; wa.qn = qn;
+  if (s.sw) {
+    const long long TR = W / 16;
+    for (int r = 0; r < 16; ++r) {
+      const long long D = (long long)((unsigned __int128)r * TR * 2 * H % n * b % n);
+      wa.colD[r] = (int)D;
+      wa.colS[r] = (double)exp2l(-(long double)D / (long double)n);
+      wa.colSi[r] = (double)exp2l((long double)D / (long double)n);
+    }
+  }
+
+  // ---- state that must start at zero: flags, ticket, error, fault
+  DevState hs{};
+  hs.offset = offset;
+  if ((e = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * (size_t)ngroups, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dst, &hs, sizeof(DevState), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dtab, g_host_tables, table_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    return LL_ERR_CUDA;
+
+  // ---- digits in -> weighted transform -> iters iterations -> digits out
+  const dim3 gw(H / s.G), gt(W / 2);
+  wa.xint = const_cast<int32_t *>(digits_in);
+  if (s.sw) s.sw->init<<<gw, s.T1, sw_bytes, st>>>(wa);
+  else wide_kernel<EPT, WIDE_INIT><<<gw, s.T1, sw_bytes, st>>>(wa);
+  if (iters == 0) {
+    e = cudaMemcpyAsync(digits_out, digits_in, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return LL_ERR_CUDA;
+  }
+  for (uint32_t i = 0; i < iters; ++i) {
+    if (s.st) s.st->run<<<gt, s.T2, st_bytes, st>>>(ta);
+    else tall_kernel<EPT><<<gt, s.T2, st_bytes, st>>>(ta);
+    const bool last = i + 1 == iters;
+    wa.xint = last ? digits_out : nullptr;
+    if (s.sw) (last ? s.sw->report : s.sw->iter)<<<gw, s.T1, sw_bytes, st>>>(wa);
+    else if (last) wide_kernel<EPT, WIDE_REPORT><<<gw, s.T1, sw_bytes, st>>>(wa);
+    else wide_kernel<EPT, WIDE_ITER><<<gw, s.T1, sw_bytes, st>>>(wa);
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return LL_ERR_CUDA;
+  if ((e = cudaMemcpyAsync(&hs, dst, sizeof(DevState), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return LL_ERR_CUDA;
+  if (max_err) memcpy(max_err, &hs.err_bits, sizeof(float));
+  if (hs.fault & 1u) return LL_ERR_TIMEOUT;
+  return LL_OK;
+}

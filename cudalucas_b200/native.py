@@ -19,6 +19,7 @@ LL_ERR_TIMEOUT = 6
 LL_ERR_INJECTED = 7
 LL_REPORT = 1
 LL_ERRCHK = 2
+LL_STATIC_MAX_WORDS = 1 << 20
 
 
 class Tuning(ctypes.Structure):
@@ -59,6 +60,7 @@ def lib():
         "ll_status_string": (ctypes.c_char_p, [i32]),
         "ll_debug_inject_failure": (None, [vp, i32]),
         "ll_debug_launch": (i32, [vp, i32]),
+        "ll_step_static": (i32, [ctypes.c_int, u32, u32, u32, u32, vp, vp, fp, vp]),
         "ll_digits_res64": (u64, [i32p, u32, u32, u32]),
         "ll_digits_standardize": (i32, [i32p, u32, u32]),
         "ll_pack_bits": (None, [i32p, u32p, u32, u32]),

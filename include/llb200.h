@@ -106,6 +106,28 @@ void ll_debug_inject_failure(ll_ctx *ctx, int32_t count);
  * iteration; used to time and profile the passes separately. */
 ll_status ll_debug_launch(ll_ctx *ctx, int32_t which);
 
+/* Allocation-free LL steps.  No counterpart in the reference: CUDALucas
+ * allocates its buffers with cudaMalloc in alloc_gpu_mem.  This entry point is
+ * for callers that cannot allocate device memory -- code running inside an
+ * arena or pool that owns all device memory, plugins whose host forbids
+ * allocation during a work call, loops that must not touch the allocator.
+ * It reads n balanced digits of x = s*2^offset from DEVICE memory digits_in,
+ * runs `iters` LL iterations and writes the digits of the result (whose
+ * offset is offset*2^iters mod q) to DEVICE memory digits_out; the max
+ * roundoff error goes to the HOST float *max_err (may be NULL).  All scratch
+ * lives in one static array of LL_STATIC_SCRATCH_BYTES per device (held by
+ * every GPU that loads the library, until exit); n may not exceed
+ * LL_STATIC_MAX_WORDS (LL_ERR_ARG otherwise).  The first call on a device
+ * looks up the array's device address; make that call before any stream
+ * capture.  Calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads' GPU work still running) race.  The call
+ * synchronises `stream` (a cudaStream_t, NULL = legacy default stream) before
+ * it returns. */
+#define LL_STATIC_MAX_WORDS (1u << 20)
+#define LL_STATIC_SCRATCH_BYTES (16u << 20)
+ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t offset, uint32_t iters,
+                         const int32_t *digits_in, int32_t *digits_out, float *max_err, void *stream);
+
 /* ------------------------------------------------------------------------
  * Host helpers (no GPU needed).  Word j of an n-word representation of
  * 2^q-1 has floor(q/n)+1 bits iff ((-j*(q mod n)) mod n) < (q mod n).
