@@ -336,18 +336,134 @@ def run_reference(args, world, rank, local):
     return base
 
 
+def run_batch(args, world, rank, local):
+    """Batched mode: 256 primes log-uniform in [1e6, 2e7] (seed 7) at the
+    length policy's FFT lengths, all advancing together (one CUDA graph per
+    step), against the same exponents run one at a time."""
+    import torch
+    import cudalucas_b200 as cl
+    from cudalucas_b200 import workloads
+    torch.cuda.set_device(local)
+    members = workloads.batch_exponents(args.batch_count, seed=7 + rank)
+    qs, ns = zip(*members)
+    S, K, W = args.iters_per_step, args.steps, args.warmup
+    b = cl.LLBatch(qs, ns, device=local, graph_iters=10)
+    b.start([(q * 7) // 11 for q in qs])
+    for _ in range(W):
+        b.step(S)
+    b.sync()
+    ext = torch.cuda.ExternalStream(b.stream, device=torch.device("cuda", local))
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        t0.record(ext)
+        for _ in range(K):
+            b.step(S)
+        t1.record(ext)
+        b.sync()
+    ms = allreduce_max(t0.elapsed_time(t1), world)
+    errs = b.step(1, report=True)
+    res = b.res64()
+    b.close()
+    # the same exponents one at a time (bounded sample of iterations each)
+    Ss = args.serial_iters
+    serial_ms = 0.0
+    for q, n in members:
+        c = cl.LLContext(q, n, device=local)
+        c.start(1)
+        c.step(20)
+        ext1 = torch.cuda.ExternalStream(c.stream, device=torch.device("cuda", local))
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(ext1)
+        c.step(Ss)
+        a1.record(ext1)
+        c.sync()
+        serial_ms += a0.elapsed_time(a1)
+        c.close()
+    serial_ms = allreduce_max(serial_ms, world)
+    if rank != 0:
+        return None
+    batch_ips = len(members) * K * S * world / (ms / 1000.0)
+    serial_ips = len(members) * Ss * world / (serial_ms / 1000.0)
+    return {
+        "metric": "batched LL iter/s (256 exponents, seed 7, 1e6..2e7)",
+        "value": round(batch_ips, 1), "unit": "iter/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": round(ms / K, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic: seeded exponents, LL tests from s0=4",
+        "config": {"workload": "batch: %d primes log-uniform in [1e6, 2e7] (seed 7), lengths %dK..%dK"
+                               % (len(members), min(ns) // 1024, max(ns) // 1024),
+                   "iters_per_step": S, "graph_iters": 10,
+                   "serial_iter_s": round(serial_ips, 1), "speedup_vs_serial": round(batch_ips / serial_ips, 3),
+                   "serial_sample": "%d iterations of each exponent alone" % Ss,
+                   "max_roundoff_error": round(float(max(errs)), 5),
+                   "res64_xor": "%016x" % (__import__("functools").reduce(lambda a, b: a ^ b, res))},
+        "clocks": clk.summary(),
+        "gpu_launches": 2 * len(members) * K * S,
+    }
+
+
+def run_serve(args, world, rank, local):
+    """Serving: Poisson arrivals at 50/s of LL requests (prime p log-uniform
+    in [1e5, 5e7], k uniform in [1e3, 5e4], seed 11), continuous batching,
+    against the same requests served one at a time in arrival order."""
+    import torch
+    from cudalucas_b200 import serve, workloads
+    torch.cuda.set_device(local)
+    reqs = workloads.serve_requests(args.serve_count, seed=11 + rank)
+
+    def mk():
+        return [serve.Request(rid=i, arrival=t, p=p, n=n, iters=k, offset=i) for i, (t, p, n, k) in enumerate(reqs)]
+    eng = serve.GpuEngine(device=local)
+    warm = mk()[:2]
+    for r in warm:
+        r.iters = 50
+    serve.Server(eng).run(warm, realtime=False)
+    barrier(world)
+    with Clocks(local) as clk:
+        batched = serve.Server(eng, chunk=args.serve_chunk).run(mk())
+    serial = serve.serve_serial(eng, mk())
+    same = all(a.res64 == b.res64 for a, b in zip(batched, serial))
+    sb, ss = serve.summary(batched), serve.summary(serial)
+    if rank != 0:
+        return None
+    return {
+        "metric": "serve p50/p99 time-to-residue (s), Poisson 50 req/s",
+        "value": round(sb["p50_s"], 4), "unit": "s", "n_gpus": world, "steps": 1, "warmup": 1,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded Poisson arrivals of LL requests",
+        "config": {"workload": "serve: %d requests, Poisson 50/s, p log-uniform [1e5, 5e7], k uniform [1e3, 5e4], "
+                               "seed 11" % len(reqs), "chunk_iters": args.serve_chunk,
+                   "continuous": sb, "serial": ss, "results_identical": same,
+                   "speedup_p50": round(ss["p50_s"] / sb["p50_s"], 3),
+                   "speedup_throughput": round(sb["iter_per_s"] / ss["iter_per_s"], 3)},
+        "p99": round(sb["p99_s"], 4),
+        "clocks": clk.summary(),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="3200K", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="3200K", choices=sorted(WORKLOADS) + ["batch", "serve"])
+    ap.add_argument("--serve-count", type=int, default=32)
+    ap.add_argument("--serve-chunk", type=int, default=1000)
+    ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--serial-iters", type=int, default=200)
     ap.add_argument("--iters-per-step", type=int, default=10000)
     ap.add_argument("--cpu-iters", type=int, default=20, help="oracle iterations for cpu_baseline (0: skip)")
     args = ap.parse_args()
     world, rank, local = dist_init()
-    if args.impl == "reference":
+    if args.workload == "serve":
+        out = run_serve(args, world, rank, local) if args.impl == "ours" else (
+            {"impl": "reference", "unavailable": "the reference has no serving mode"} if rank == 0 else None)
+    elif args.workload == "batch":
+        out = run_batch(args, world, rank, local) if args.impl == "ours" else (
+            {"impl": "reference", "unavailable": "the reference has no batched mode"} if rank == 0 else None)
+    elif args.impl == "reference":
         out = run_reference(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)

@@ -614,6 +614,10 @@ struct ll_ctx {
   std::string err;
   TallArgs ta{};
   WideArgs wa{};
+  // CUDA graph of `graph_iters` plain iterations, captured on first use
+  int graph_iters = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
 };
 
 static ll_status cuda_fail(ll_ctx *c, cudaError_t e, const char *what) {
@@ -645,6 +649,8 @@ static void free_ctx(ll_ctx *c) {
                   c->rowE, c->colF, c->rowW, c->rowWi, c->colW, c->colWi};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->graph) cudaGraphDestroy(c->graph);
   if (c->stream) cudaStreamDestroy(c->stream);
   cudaSetDevice(prev);
   delete c;
@@ -734,6 +740,8 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
   ctx->qn = q / n;
   ctx->N = (int)(n / 2);
   ctx->shape = s;
+  ctx->graph_iters = tuning && tuning->graph_iters > 0 ? tuning->graph_iters : 64;
+  if (tuning && tuning->graph_iters < 0) ctx->graph_iters = 0;  // graphs disabled
   if (ctx->qn + 1 > 30) { delete ctx; return LL_ERR_ARG; }
   make_plan(s.W, ctx->pw);
   make_plan(s.H, ctx->ph);
@@ -898,7 +906,30 @@ ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
   }
   CK(cudaSetDevice(ctx->device));
   const bool report = (flags & LL_REPORT) != 0;
-  for (uint32_t i = 0; i < iters; ++i) {
+  uint32_t done = 0;
+  const uint32_t K = (uint32_t)ctx->graph_iters;
+  if (K && iters >= K + (report ? 1u : 0u)) {
+    // iterations without a report, K at a time, replayed from one CUDA graph
+    if (!ctx->graph_exec) {
+      CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      const uint32_t off0 = ctx->offset;
+      for (uint32_t i = 0; i < K; ++i) {
+        launch_tall(ctx);
+        launch_wide(ctx, WIDE_ITER);
+      }
+      ctx->offset = off0;
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &ctx->graph);
+      if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+      CK(cudaGraphInstantiate(&ctx->graph_exec, ctx->graph, 0));
+    }
+    const uint32_t plain = iters - (report ? 1u : 0u);
+    while (plain - done >= K) {
+      CK(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+      for (uint32_t i = 0; i < K; ++i) ctx->offset = (uint32_t)((2ull * ctx->offset) % ctx->q);
+      done += K;
+    }
+  }
+  for (uint32_t i = done; i < iters; ++i) {
     ll_status rc = launch_iteration(ctx, report && i + 1 == iters);
     if (rc != LL_OK) return rc;
   }
@@ -926,6 +957,16 @@ ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
     }
   }
   return LL_OK;
+}
+
+int32_t ll_busy(ll_ctx *ctx) {
+  if (!ctx) return -1;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return -1;
+  const cudaError_t e = cudaStreamQuery(ctx->stream);
+  if (e == cudaSuccess) return 0;
+  if (e == cudaErrorNotReady) return 1;
+  ctx->err = cudaGetErrorString(e);
+  return -1;
 }
 
 ll_status ll_sync(ll_ctx *ctx) {
@@ -1209,3 +1250,172 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
   if (hs.fault & 1u) return LL_ERR_TIMEOUT;
   return LL_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Batched mode: many exponents of any lengths advance together.
+//
+// Every member is an ordinary context (own buffers, tables, stream and
+// shape).  One step of K iterations for the whole batch is a single CUDA
+// graph: each member's chain of K x (tall, wide) launches is its own branch,
+// the branches fork from and join back to the batch stream, and the GPU runs
+// the independent branches concurrently.  A member runs exactly the kernels it
+// would run alone, so its residues are the solo residues.
+struct ll_batch {
+  int device = 0;
+  std::vector<ll_ctx *> members;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaEvent_t> events;  // [0] fork, [1..] joins
+  int graph_iters = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  std::string err;
+};
+
+static void free_batch(ll_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  for (ll_ctx *c : b->members) ll_destroy(c);
+  delete b;
+}
+
+extern "C" {
+
+ll_status ll_batch_create(int device, int32_t count, const uint32_t *q, const uint32_t *n, int32_t graph_iters,
+                          ll_batch **out) {
+  if (!out || count <= 0 || !q || !n) return LL_ERR_ARG;
+  *out = nullptr;
+  ll_batch *b = new ll_batch();
+  b->device = device;
+  b->graph_iters = graph_iters > 0 ? graph_iters : 10;
+  ll_tuning t{};
+  t.graph_iters = -1;  // members never capture their own graphs
+  for (int32_t i = 0; i < count; ++i) {
+    ll_ctx *c = nullptr;
+    ll_status s = ll_create(device, q[i], n[i], &t, &c);
+    if (s != LL_OK) {
+      free_batch(b);
+      return s;
+    }
+    b->members.push_back(c);
+  }
+  cudaSetDevice(device);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    free_batch(b);
+    return LL_ERR_CUDA;
+  }
+  b->events.resize((size_t)count + 1, nullptr);
+  for (auto &e : b->events)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      free_batch(b);
+      return LL_ERR_CUDA;
+    }
+  *out = b;
+  return LL_OK;
+}
+
+void ll_batch_destroy(ll_batch *b) { free_batch(b); }
+
+int32_t ll_batch_size(const ll_batch *b) { return b ? (int32_t)b->members.size() : 0; }
+
+ll_ctx *ll_batch_member(ll_batch *b, int32_t i) {
+  if (!b || i < 0 || i >= (int32_t)b->members.size()) return nullptr;
+  return b->members[(size_t)i];
+}
+
+ll_status ll_batch_start(ll_batch *b, const uint32_t *offsets) {
+  if (!b) return LL_ERR_ARG;
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    ll_status s = ll_start(b->members[i], offsets ? offsets[i] : 0);
+    if (s != LL_OK) return s;
+  }
+  return LL_OK;
+}
+
+ll_status ll_batch_step(ll_batch *b, uint32_t iters, uint32_t flags, float *max_err) {
+  if (!b) return LL_ERR_ARG;
+  for (ll_ctx *c : b->members)
+    if (!c->started) return LL_ERR_STATE;
+  if (cudaSetDevice(b->device) != cudaSuccess) return LL_ERR_CUDA;
+  const bool report = (flags & LL_REPORT) != 0;
+  const uint32_t K = (uint32_t)b->graph_iters;
+  const uint32_t plain = iters - (report && iters ? 1u : 0u);
+  uint32_t done = 0;
+  if (plain >= K) {
+    if (!b->graph_exec) {
+      if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return LL_ERR_CUDA;
+      cudaEventRecord(b->events[0], b->stream);
+      for (size_t i = 0; i < b->members.size(); ++i) {
+        ll_ctx *c = b->members[i];
+        cudaStreamWaitEvent(c->stream, b->events[0], 0);
+        const uint32_t off0 = c->offset;
+        for (uint32_t k = 0; k < K; ++k) {
+          launch_tall(c);
+          launch_wide(c, WIDE_ITER);
+        }
+        c->offset = off0;
+        cudaEventRecord(b->events[i + 1], c->stream);
+        cudaStreamWaitEvent(b->stream, b->events[i + 1], 0);
+      }
+      cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
+      if (e != cudaSuccess) {
+        b->err = cudaGetErrorString(e);
+        return LL_ERR_CUDA;
+      }
+      if (cudaGraphInstantiate(&b->graph_exec, b->graph, 0) != cudaSuccess) return LL_ERR_CUDA;
+    }
+    // the members' streams must have finished earlier work (e.g. ll_start)
+    for (ll_ctx *c : b->members) {
+      cudaEvent_t ev = b->events[0];
+      cudaEventRecord(ev, c->stream);
+      cudaStreamWaitEvent(b->stream, ev, 0);
+    }
+    while (plain - done >= K) {
+      if (cudaGraphLaunch(b->graph_exec, b->stream) != cudaSuccess) return LL_ERR_CUDA;
+      for (ll_ctx *c : b->members)
+        for (uint32_t k = 0; k < K; ++k) c->offset = (uint32_t)((2ull * c->offset) % c->q);
+      done += K;
+    }
+    // later per-member work is ordered after the graph
+    cudaEventRecord(b->events[0], b->stream);
+    for (ll_ctx *c : b->members) cudaStreamWaitEvent(c->stream, b->events[0], 0);
+  }
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    ll_ctx *c = b->members[i];
+    float e = 0.f;
+    const uint32_t rest = iters - done;
+    if (rest || flags) {
+      ll_status s = ll_step(c, rest, flags, &e);
+      if (s != LL_OK) return s;
+    } else if (iters) {
+      c->digits_current = false;
+    }
+    if (max_err) max_err[i] = e;
+  }
+  return LL_OK;
+}
+
+void *ll_batch_stream(const ll_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+ll_status ll_batch_sync(ll_batch *b) {
+  if (!b) return LL_ERR_ARG;
+  cudaSetDevice(b->device);
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) return LL_ERR_CUDA;
+  for (ll_ctx *c : b->members)
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return LL_ERR_CUDA;
+  return LL_OK;
+}
+
+ll_status ll_batch_res64(ll_batch *b, uint64_t *res64) {
+  if (!b || !res64) return LL_ERR_ARG;
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    ll_status s = ll_res64(b->members[i], &res64[i]);
+    if (s != LL_OK) return s;
+  }
+  return LL_OK;
+}
+
+}  // extern "C"

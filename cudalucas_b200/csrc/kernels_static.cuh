@@ -188,6 +188,15 @@ constexpr int min_blocks(int threads) { return 65536 / (threads * 128) > 1 ? 655
 // Shared memory of the tall pass beyond the two columns: stage twiddles,
 // the column twiddle factors w_N^(k*TR*r) of both columns (2 x 16) and the
 // pairing-loop factors w_H^(j*2*TR) (8 entries).
+// 16-byte asynchronous global -> shared copy (no register staging).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
 template <class P>
 __host__ __device__ constexpr int tall_extra() { return tw_size<P>() + 32 + 8; }
 
@@ -214,7 +223,7 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
     const uint32_t o = a.st->offset;  // CUDALucas.cu:1882, once per iteration
     a.st->offset = (uint32_t)((2ull * o) % a.q);
   }
-  for (int i = threadIdx.x; i < tw_size<P>(); i += T) stw[i] = a.stw[i];
+  for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
   if (threadIdx.x < 32) {
     const int kk = threadIdx.x < 16 ? kA : kB, r = threadIdx.x & 15;
     wr[threadIdx.x] = omegaN(a.thi, a.tlo, a.ts, a.tmask, kk * TR * r);
@@ -222,12 +231,15 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
     pj[threadIdx.x - 32] = __ldg(&a.twH[(threadIdx.x - 32) * T]);
   }
   const double2 base = omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * t);
-  __syncthreads();
   const double2 *src = a.A + (size_t)k1 * H;
   {
     double2 v[16];
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = cmul(src[t + r * TR], cmul(base, wr[col * 16 + r]));
+    for (int r = 0; r < 16; ++r) v[r] = src[t + r * TR];
+    cp_async_wait_all();
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = cmul(v[r], cmul(base, wr[col * 16 + r]));
     first_stage_from_regs<H, TR>(sm, v, col, t);
   }
   __syncthreads();
@@ -282,15 +294,6 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
 
 template <class P, int G>
 constexpr int wide_threads() { return G * (P::L / 16); }
-
-// 16-byte asynchronous global -> shared copy (no register staging).
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
-}
 
 // Splits an integer-valued double v (|v| < 2^52) as v = h*2^b + l, 0 <= l < 2^b
 // (exact: scaling by powers of two and floor are exact in FP64).

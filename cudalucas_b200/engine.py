@@ -88,6 +88,12 @@ class LLContext:
     def sync(self):
         self._check(native.lib().ll_sync(self._h), "ll_sync")
 
+    def busy(self):
+        r = native.lib().ll_busy(self._h)
+        if r < 0:
+            raise LLError(native.LL_ERR_CUDA, "ll_busy")
+        return bool(r)
+
     def debug_launch(self, which):
         self._check(native.lib().ll_debug_launch(self._h, int(which)), "ll_debug_launch")
 
@@ -107,6 +113,70 @@ class LLContext:
         v = [ctypes.c_int32() for _ in range(5)]
         native.lib().ll_shape(self._h, *[ctypes.byref(x) for x in v])
         return dict(zip(("W", "H", "G", "threads_wide", "threads_tall"), [x.value for x in v]))
+
+
+class LLBatch:
+    """Many exponents advancing together (ll_batch_* in include/llb200.h)."""
+
+    def __init__(self, qs, ns, device=0, graph_iters=10):
+        L = native.lib()
+        self.qs = [int(x) for x in qs]
+        self.ns = [int(x) for x in ns]
+        q = np.ascontiguousarray(self.qs, dtype=np.uint32)
+        n = np.ascontiguousarray(self.ns, dtype=np.uint32)
+        self._h = ctypes.c_void_p()
+        rc = L.ll_batch_create(int(device), len(self.qs), _u32p(q), _u32p(n), int(graph_iters),
+                               ctypes.byref(self._h))
+        if rc:
+            raise LLError(rc, "ll_batch_create")
+        self._keep = (q, n)
+
+    def close(self):
+        if self._h:
+            native.lib().ll_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    __del__ = close
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return len(self.qs)
+
+    def start(self, offsets=None):
+        o = np.ascontiguousarray(offsets if offsets is not None else [0] * len(self), dtype=np.uint32)
+        rc = native.lib().ll_batch_start(self._h, _u32p(o))
+        if rc:
+            raise LLError(rc, "ll_batch_start")
+
+    def step(self, iters, report=False, errchk=False):
+        flags = (LL_REPORT if report else 0) | (LL_ERRCHK if errchk else 0)
+        errs = np.zeros(len(self), dtype=np.float32)
+        rc = native.lib().ll_batch_step(self._h, int(iters), flags,
+                                        errs.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        if rc:
+            raise LLError(rc, "ll_batch_step")
+        return errs if flags else None
+
+    @property
+    def stream(self):
+        return native.lib().ll_batch_stream(self._h)
+
+    def sync(self):
+        rc = native.lib().ll_batch_sync(self._h)
+        if rc:
+            raise LLError(rc, "ll_batch_sync")
+
+    def res64(self):
+        out = np.zeros(len(self), dtype=np.uint64)
+        rc = native.lib().ll_batch_res64(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+        if rc:
+            raise LLError(rc, "ll_batch_res64")
+        return [int(x) for x in out]
 
 
 # ---- host helpers (no GPU) -------------------------------------------------

@@ -51,6 +51,7 @@ def lib():
         "ll_read_digits": (i32, [vp, i32p, u32p]),
         "ll_res64": (i32, [vp, ctypes.POINTER(u64)]),
         "ll_sync": (i32, [vp]),
+        "ll_busy": (i32, [vp]),
         "ll_exponent": (u32, [vp]),
         "ll_fft_length": (u32, [vp]),
         "ll_offset": (u32, [vp]),
@@ -61,6 +62,15 @@ def lib():
         "ll_debug_inject_failure": (None, [vp, i32]),
         "ll_debug_launch": (i32, [vp, i32]),
         "ll_step_static": (i32, [ctypes.c_int, u32, u32, u32, u32, vp, vp, fp, vp]),
+        "ll_batch_create": (i32, [ctypes.c_int, i32, u32p, u32p, i32, ctypes.POINTER(vp)]),
+        "ll_batch_destroy": (None, [vp]),
+        "ll_batch_size": (i32, [vp]),
+        "ll_batch_member": (vp, [vp, i32]),
+        "ll_batch_start": (i32, [vp, u32p]),
+        "ll_batch_step": (i32, [vp, u32, u32, fp]),
+        "ll_batch_sync": (i32, [vp]),
+        "ll_batch_stream": (vp, [vp]),
+        "ll_batch_res64": (i32, [vp, ctypes.POINTER(u64)]),
         "ll_digits_res64": (u64, [i32p, u32, u32, u32]),
         "ll_digits_standardize": (i32, [i32p, u32, u32]),
         "ll_pack_bits": (None, [i32p, u32p, u32, u32]),

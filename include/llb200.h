@@ -87,6 +87,10 @@ ll_status ll_res64(ll_ctx *ctx, uint64_t *res64);
 /* Waits for all queued work of the context. */
 ll_status ll_sync(ll_ctx *ctx);
 
+/* Non-blocking: 1 while queued work of the context is still running, 0 when
+ * it is idle, -1 on a CUDA error (the serving loop polls with this). */
+int32_t ll_busy(ll_ctx *ctx);
+
 /* Properties of a context. */
 uint32_t ll_exponent(const ll_ctx *ctx);
 uint32_t ll_fft_length(const ll_ctx *ctx);
@@ -105,6 +109,27 @@ void ll_debug_inject_failure(ll_ctx *ctx, int32_t count);
 /* Launches only the tall pass (square) or only the wide pass (carry) of one
  * iteration; used to time and profile the passes separately. */
 ll_status ll_debug_launch(ll_ctx *ctx, int32_t which);
+
+/* Batched mode (no counterpart in the reference, which tests one exponent per
+ * process): `count` exponents q[i] at lengths n[i] advance together.  Each
+ * member is a full context (ll_batch_member gives it for ll_load_digits,
+ * ll_read_digits, ...); one step of `graph_iters` iterations of all members is
+ * replayed from a single CUDA graph in which every member is a parallel
+ * branch, so members of different lengths overlap on the GPU.  A member runs
+ * exactly the kernels of a solo run: its residues equal the solo residues. */
+typedef struct ll_batch ll_batch;
+ll_status ll_batch_create(int device, int32_t count, const uint32_t *q, const uint32_t *n, int32_t graph_iters,
+                          ll_batch **out);
+void ll_batch_destroy(ll_batch *b);
+int32_t ll_batch_size(const ll_batch *b);
+ll_ctx *ll_batch_member(ll_batch *b, int32_t i);
+ll_status ll_batch_start(ll_batch *b, const uint32_t *offsets);
+/* iters iterations of every member; flags as ll_step (applied to each
+ * member's last iteration); max_err[i] per member when a flag is given. */
+ll_status ll_batch_step(ll_batch *b, uint32_t iters, uint32_t flags, float *max_err);
+ll_status ll_batch_sync(ll_batch *b);
+void *ll_batch_stream(const ll_batch *b);  /* stream the step graphs run on */
+ll_status ll_batch_res64(ll_batch *b, uint64_t *res64);
 
 /* Allocation-free LL steps.  No counterpart in the reference: CUDALucas
  * allocates its buffers with cudaMalloc in alloc_gpu_mem.  This entry point is
