@@ -86,6 +86,7 @@ struct WideArgs {
   // (mod n), i.e. weight colW[t] * colS[r] (times 2 when it wraps)
   int colD[16];
   double colS[16], colSi[16];
+  double colS2[16], colSi2[16];  // 2*colS, 0.5*colSi (wrapped exponents)
 };
 
 __device__ __forceinline__ double2 omegaN(const double2 *__restrict__ thi, const double2 *__restrict__ tlo,
@@ -816,6 +817,8 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
         wa.colD[r] = (int)D;
         wa.colS[r] = (double)exp2l(-(long double)D / (long double)n);
         wa.colSi[r] = (double)exp2l((long double)D / (long double)n);
+        wa.colS2[r] = 2.0 * wa.colS[r];
+        wa.colSi2[r] = 0.5 * wa.colSi[r];
       }
     }
   } while (0);
@@ -1213,6 +1216,8 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
       wa.colD[r] = (int)D;
       wa.colS[r] = (double)exp2l(-(long double)D / (long double)n);
       wa.colSi[r] = (double)exp2l((long double)D / (long double)n);
+      wa.colS2[r] = 2.0 * wa.colS[r];
+      wa.colSi2[r] = 0.5 * wa.colSi[r];
     }
   }
 

@@ -333,25 +333,40 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   const int row = threadIdx.x / TR, t = threadIdx.x - row * TR;
   const int m2 = m2b + row;
   const int n = (int)a.n, bb = (int)a.b, qn = (int)a.qn;
-  // per-row and per-thread weight bases (word 2*m2+s, column t)
-  const int eR0 = __ldg(&a.rowE[2 * m2]), eR1 = __ldg(&a.rowE[2 * m2 + 1]);
-  const double rw0 = __ldg(&a.rowW[2 * m2]), rw1 = __ldg(&a.rowW[2 * m2 + 1]);
-  const int ft = __ldg(&a.colF[t]);
+  // Word s (0, 1) of element (m1 = t + r*TR, m2) has weight exponent
+  // e = (E_s - colD[r]) mod n with the per-thread E_s = rowE + colF[t] mod n,
+  // so its weight is Wt_s * colS[r] (or * colS2[r] when E_s < colD[r]).
+  int E0 = __ldg(&a.rowE[2 * m2]) + __ldg(&a.colF[t]);
+  int E1 = __ldg(&a.rowE[2 * m2 + 1]) + __ldg(&a.colF[t]);
   const double cwt = __ldg(&a.colW[t]);
+  const double W0 = __ldg(&a.rowW[2 * m2]) * cwt * (E0 >= n ? 0.5 : 1.0);
+  const double W1 = __ldg(&a.rowW[2 * m2 + 1]) * cwt * (E1 >= n ? 0.5 : 1.0);
+  if (E0 >= n) E0 -= n;
+  if (E1 >= n) E1 -= n;
   const double p2lo = (double)(1 << qn), p2hi = 2.0 * p2lo;
   const double ip2lo = 1.0 / p2lo, ip2hi = 0.5 * ip2lo;
   double2 x[16];
-  float emax = 0.f;
+  double emax = 0.0;
   uint32_t fault = 0;
 
   if (MODE != WIDE_INIT) {
-    const double rwi0 = __ldg(&a.rowWi[2 * m2]), rwi1 = __ldg(&a.rowWi[2 * m2 + 1]);
     const double cwit = __ldg(&a.colWi[t]);
+    const double Wi0 = __ldg(&a.rowWi[2 * m2]) * cwit * (__ldg(&a.rowE[2 * m2]) + __ldg(&a.colF[t]) >= n ? 2.0 : 1.0);
+    const double Wi1 =
+        __ldg(&a.rowWi[2 * m2 + 1]) * cwit * (__ldg(&a.rowE[2 * m2 + 1]) + __ldg(&a.colF[t]) >= n ? 2.0 : 1.0);
+    // the -2 (bit (offset+1) mod q, CUDALucas.cu:1882-1886) hits at most one
+    // word; locate it once: element register r_sub, word w_sub
     const uint32_t off = a.st->offset;
     const uint32_t pos = (off + 1) % a.q;
     const uint32_t dw = (uint32_t)(((unsigned long long)pos * a.n) / a.q);
     const uint32_t sdw = (uint32_t)(((unsigned long long)dw * a.q + a.n - 1) / a.n);
     const double sub = (double)(1u << (pos - sdw));
+    int r_sub = -1;
+    {
+      const uint32_t me = dw >> 1, mm1 = me / (uint32_t)H, mm2 = me - mm1 * (uint32_t)H;
+      if ((int)mm2 == m2 && (int)(mm1 % TR) == t) r_sub = (int)(mm1 / TR);
+    }
+    const bool w_sub = dw & 1;
     cp_async_wait_all();
     __syncthreads();
     inv_stages<P, 0, P::N - 1, 1, TR>(sm, stw, row, t);
@@ -366,20 +381,18 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
-      const int fr = ft - a.colD[r];
-      const bool fw = fr < 0;
-      const int f = fw ? fr + n : fr;
-      const double cwi = cwit * a.colSi[r] * (fw ? 0.5 : 1.0);
-      const int e0 = eR0 + f, e1 = eR1 + f;
-      const bool w0 = e0 >= n, w1 = e1 >= n;
-      const double t0 = u[r].x * (rwi0 * cwi * (w0 ? 2.0 : 1.0));
-      const double t1 = u[r].y * (rwi1 * cwi * (w1 ? 2.0 : 1.0));
+      const int D = a.colD[r];
+      const bool n0 = E0 < D, n1 = E1 < D;
+      const int e0 = E0 - D + (n0 ? n : 0), e1 = E1 - D + (n1 ? n : 0);
+      const double t0 = u[r].x * (Wi0 * (n0 ? a.colSi2[r] : a.colSi[r]));
+      const double t1 = u[r].y * (Wi1 * (n1 ? a.colSi2[r] : a.colSi[r]));
       double r0 = rint(t0), r1 = rint(t1);
-      emax = fmaxf(emax, fmaxf(fabsf((float)(t0 - r0)), fabsf((float)(t1 - r1))));
-      const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
-      if (j0 == dw) r0 -= sub;
-      if (j0 + 1 == dw) r1 -= sub;
-      const bool big0 = (w0 ? e0 - n : e0) < bb, big1 = (w1 ? e1 - n : e1) < bb;
+      emax = fmax(emax, fmax(fabs(t0 - r0), fabs(t1 - r1)));
+      if (r == r_sub) {
+        if (w_sub) r1 -= sub;
+        else r0 -= sub;
+      }
+      const bool big0 = e0 < bb, big1 = e1 < bb;
       const double P1 = big1 ? p2hi : p2lo, I1 = big1 ? ip2hi : ip2lo;
       // word i keeps bal(low_i + c1_{i-1}) + c2_{i-1}: c1 is the high part of
       // the previous word, c2 the carry out of balancing the previous word
@@ -395,7 +408,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
       cs[row * W + m1] = pc;
       if (row == G - 1) gc[(size_t)g * W + m1] = pc;
     }
-    __threadfence();
+    if (row == G - 1) __threadfence();
     __syncthreads();
     const int pred = g == 0 ? a.ngroups - 1 : g - 1;
     if (threadIdx.x == 0) {
@@ -413,13 +426,10 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
         const long long raw = __ldcg(&a.carry[(size_t)pred * W + (g == 0 ? (m1 == 0 ? W - 1 : m1 - 1) : m1)]);
         cin = make_int2((int)(raw & 0xffffffffll), (int)(raw >> 32));
       }
-      const int fr = ft - a.colD[r];
-      const bool fw = fr < 0;
-      const int f = fw ? fr + n : fr;
-      const double cw = cwt * a.colS[r] * (fw ? 2.0 : 1.0);
-      const int e0 = eR0 + f, e1 = eR1 + f;
-      const bool w0 = e0 >= n, w1 = e1 >= n;
-      const bool big0 = (w0 ? e0 - n : e0) < bb;
+      const int D = a.colD[r];
+      const bool n0 = E0 < D, n1 = E1 < D;
+      const int e0 = E0 - D + (n0 ? n : 0);
+      const bool big0 = e0 < bb;
       const double P0 = big0 ? p2hi : p2lo, I0 = big0 ? ip2hi : ip2lo;
       const double tt0 = (double)keep[r].x + (double)cin.x;
       const double k0 = floor((tt0 + 0.5 * P0) * I0);
@@ -430,7 +440,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
         a.xint[j0] = (int32_t)d0;
         a.xint[j0 + 1] = (int32_t)d1;
       }
-      x[r] = make_double2(d0 * (rw0 * cw * (w0 ? 0.5 : 1.0)), d1 * (rw1 * cw * (w1 ? 0.5 : 1.0)));
+      x[r] = make_double2(d0 * (W0 * (n0 ? a.colS2[r] : a.colS[r])), d1 * (W1 * (n1 ? a.colS2[r] : a.colS[r])));
     }
     __syncthreads();  // carry reads done before the data region is rewritten
   } else {
@@ -439,14 +449,11 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
-      const int fr = ft - a.colD[r];
-      const bool fw = fr < 0;
-      const int f = fw ? fr + n : fr;
-      const double cw = cwt * a.colS[r] * (fw ? 2.0 : 1.0);
-      const int e0 = eR0 + f, e1 = eR1 + f;
+      const int D = a.colD[r];
+      const bool n0 = E0 < D, n1 = E1 < D;
       const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
-      x[r] = make_double2((double)a.xint[j0] * (rw0 * cw * (e0 >= n ? 0.5 : 1.0)),
-                          (double)a.xint[j0 + 1] * (rw1 * cw * (e1 >= n ? 0.5 : 1.0)));
+      x[r] = make_double2((double)a.xint[j0] * (W0 * (n0 ? a.colS2[r] : a.colS[r])),
+                          (double)a.xint[j0 + 1] * (W1 * (n1 ? a.colS2[r] : a.colS[r])));
     }
   }
   first_stage_from_regs<W, TR>(sm, x, row, t);
@@ -458,8 +465,9 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   }
   if (MODE != WIDE_INIT) {
 #pragma unroll
-    for (int o = 16; o; o >>= 1) emax = fmaxf(emax, __shfl_xor_sync(0xffffffffu, emax, o));
-    if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = emax;
+    float em = (float)emax;
+    for (int o = 16; o; o >>= 1) em = fmaxf(em, __shfl_xor_sync(0xffffffffu, em, o));
+    if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = em;
     if (fault) atomicOr(&s_fault, fault);
     __syncthreads();
     if (threadIdx.x == 0) {
