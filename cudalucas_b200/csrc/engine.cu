@@ -572,15 +572,18 @@ size_t shape_tall_smem(const Shape &s) {
 }
 
 // Stage twiddles of a radix list in the order the specialised kernels read
-// them: for each stage with NS > 1, rows k < NS of w_{NS*R}^(r*k), r = 1..R-1.
+// them: for each stage with NS > 1, rows k < NS of w_{NS*R}^(r*k), r = 1..R-1,
+// each row padded to an odd length (tw_stride in kernels_static.cuh).
 std::vector<double2> stage_twiddles(const int *rad, int nrad) {
   std::vector<double2> out;
   long long ns = 1;
   for (int i = 0; i < nrad; ++i) {
     const int R = rad[i];
     if (ns > 1)
-      for (long long k = 0; k < ns; ++k)
+      for (long long k = 0; k < ns; ++k) {
         for (int r = 1; r < R; ++r) out.push_back(unit_root((unsigned long long)(r * k), (unsigned long long)(ns * R)));
+        if ((R - 1) % 2 == 0) out.push_back(make_double2(0.0, 0.0));
+      }
     ns *= R;
   }
   return out;
@@ -1155,7 +1158,10 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
       const int R = rad[i];
       if (ns > 1)
         for (long long kk = 0; kk < ns; ++kk)
+        {
           for (int r = 1; r < R; ++r) out[k++] = unit_root((unsigned long long)(r * kk), (unsigned long long)(ns * R));
+          if ((R - 1) % 2 == 0) out[k++] = make_double2(0.0, 0.0);  // odd row stride (bank spread)
+        }
       ns *= R;
     }
     return k;

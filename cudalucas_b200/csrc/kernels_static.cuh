@@ -74,13 +74,17 @@ __device__ __forceinline__ constexpr int sslot(int r) {
 // Stage twiddles live in one table per row length, in stage order: for
 // every stage s with NS_s > 1 (radices of the list a[] applied in order,
 // NS_s = a[0]*...*a[s-1]) the entries w_{NS_s*R_s}^(r*k) for k < NS_s,
-// r = 1..R_s-1, row k contiguous.  The lists used are palindromic, so the
-// reversed (inverse) order has the same stages and uses the same table.
+// r = 1..R_s-1, row k contiguous with an odd row stride (R-1 rounded up to
+// odd) so that consecutive k fall in distinct shared-memory bank groups.
+// The lists used are palindromic, so the reversed (inverse) order has the
+// same stages and uses the same table.
+__host__ __device__ constexpr int tw_stride(int R) { return (R - 1) | 1; }
+
 template <class P, int I>
 __host__ __device__ constexpr int tw_offset() {
   int off = 0, ns = 1;
   for (int i = 0; i < I; ++i) {
-    if (ns > 1) off += ns * (P::a[i] - 1);
+    if (ns > 1) off += ns * tw_stride(P::a[i]);
     ns *= P::a[i];
   }
   return off;
@@ -114,7 +118,7 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, i
         const int k = j % NS;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          const double2 w = tw[k * (R - 1) + r - 1];
+          const double2 w = tw[k * tw_stride(R) + r - 1];
           v[b][r] = SIGN > 0 ? cmul(v[b][r], w) : cmulc(v[b][r], w);
         }
       }
