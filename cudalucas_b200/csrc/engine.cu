@@ -24,7 +24,15 @@
 // element m's own two words, so the carry from the last row of CTA g to the
 // first row of CTA g+1 (and from the top word to word 0, the 2^q == 1 wrap of
 // carry_out[(blk+1) mod grid], CUDALucas.cu:474-483) is published once and
-// read once: a single bounded wait per CTA, no serial chain.
+// read once: a single bounded wait per CTA, no serial chain.  (The generic
+// kernels below hand over the pair packed in an int64; the specialised ones
+// in kernels_static.cuh hand over the sum c1 + c2 as one double, which adds
+// c2 before instead of after balancing word 0 -- the same value.)
+//
+// Consecutive passes are chained with programmatic dependent launch when a
+// pass runs in a few waves: the next kernel's CTAs load their constant tables
+// while the previous pass drains, and wait (griddepcontrol.wait) before they
+// touch the state.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -363,6 +371,7 @@ struct StaticWide {
   void (*init)(WideArgs);
   int nrad, rad[4];
   int extra;  // shared-memory entries beyond the rows (stage twiddles)
+  int rows;   // shared-memory entries of the G rows
 };
 struct StaticTall {
   int L;
@@ -373,7 +382,8 @@ struct StaticTall {
 
 #define LLB_WIDE(LIST, G)                                                                                       \
   {LIST::L, G, wide_static<LIST, G, WIDE_ITER>, wide_static<LIST, G, WIDE_REPORT>, wide_static<LIST, G, WIDE_INIT>, \
-   LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tw_size<LIST>()}
+   LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tw_size<LIST>(),             \
+   G * row_slots<LIST::L, G>()}
 #define LLB_TALL(LIST) \
   {LIST::L, tall_static<LIST>, LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tall_extra<LIST>()}
 
@@ -565,7 +575,8 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
 }
 
 size_t shape_wide_smem(const Shape &s) {
-  return wide_smem(s.W, s.G) + (s.sw ? sizeof(double2) * (size_t)s.sw->extra : 0);
+  if (s.sw) return sizeof(double2) * (size_t)(s.sw->rows + s.sw->extra);
+  return wide_smem(s.W, s.G);
 }
 size_t shape_tall_smem(const Shape &s) {
   return tall_smem(s.H) + (s.st ? sizeof(double2) * (size_t)s.st->extra : 0);
@@ -614,6 +625,7 @@ struct ll_ctx {
   bool digits_current = false;
   bool started = false;
   int inject = 0;
+  bool pdl = false;  // chain the passes with programmatic dependent launch
   float pending_err = 0.f;
   std::string err;
   TallArgs ta{};
@@ -803,6 +815,20 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
       max_sw = sw;
       max_st = st;
     }
+    // Programmatic dependent launch pays when a pass runs in a few waves (the
+    // next pass's prologue overlaps this one's drain); with many waves it
+    // measured slower, so it is used only up to four waves per pass.
+    if (s.sw && s.st) {
+      int sms = 0, bw = 0, bt = 0;
+      if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bw, s.sw->iter, s.T1, shape_wide_smem(s)) == cudaSuccess &&
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, s.st->run, s.T2, shape_tall_smem(s)) == cudaSuccess &&
+          bw > 0 && bt > 0) {
+        const long long ww = ((long long)(s.H / s.G) + (long long)sms * bw - 1) / ((long long)sms * bw);
+        const long long wt = ((long long)(s.W / 2) + (long long)sms * bt - 1) / ((long long)sms * bt);
+        ctx->pdl = ww <= 4 && wt <= 4;
+      }
+    }
     TallArgs &ta = ctx->ta;
     ta.A = ctx->A; ta.stw = ctx->stwH; ta.twH = ctx->twH; ta.thi = ctx->thi; ta.tlo = ctx->tlo; ta.st = ctx->st;
     ta.ph = ctx->ph; ta.W = s.W; ta.H = s.H; ta.N = ctx->N; ta.ts = ctx->ts; ta.tmask = (1 << ctx->ts) - 1; ta.q = q;
@@ -836,12 +862,32 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
 
 void ll_destroy(ll_ctx *ctx) { free_ctx(ctx); }
 
-static void launch_wide(ll_ctx *ctx, int mode) {
+// Launches a specialised pass.  `chained`: the previous operation in the
+// stream is the other pass, so the launch may use programmatic stream
+// serialization (the kernel runs its prologue while that pass drains and
+// waits in griddep_wait() before touching the state).
+static void launch_static(const void *k, void *args, int grid, int threads, size_t smem, cudaStream_t st,
+                          bool chained) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = chained ? 1 : 0;
+  void *argv[] = {args};
+  cudaLaunchKernelExC(&cfg, k, argv);
+}
+
+static void launch_wide(ll_ctx *ctx, int mode, bool chained = false) {
   const Shape &s = ctx->shape;
   const size_t sm = shape_wide_smem(s);
   if (s.sw) {
     void (*k)(WideArgs) = mode == WIDE_INIT ? s.sw->init : mode == WIDE_REPORT ? s.sw->report : s.sw->iter;
-    k<<<s.H / s.G, s.T1, sm, ctx->stream>>>(ctx->wa);
+    launch_static((const void *)k, &ctx->wa, s.H / s.G, s.T1, sm, ctx->stream, chained && ctx->pdl);
   } else if (mode == WIDE_INIT) {
     wide_kernel<EPT, WIDE_INIT><<<s.H / s.G, s.T1, sm, ctx->stream>>>(ctx->wa);
   } else if (mode == WIDE_REPORT) {
@@ -851,9 +897,9 @@ static void launch_wide(ll_ctx *ctx, int mode) {
   }
 }
 
-static void launch_tall(ll_ctx *ctx) {
+static void launch_tall(ll_ctx *ctx, bool chained = false) {
   const Shape &s = ctx->shape;
-  if (s.st) s.st->run<<<s.W / 2, s.T2, shape_tall_smem(s), ctx->stream>>>(ctx->ta);
+  if (s.st) launch_static((const void *)s.st->run, &ctx->ta, s.W / 2, s.T2, shape_tall_smem(s), ctx->stream, chained && ctx->pdl);
   else tall_kernel<EPT><<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
 }
 
@@ -896,7 +942,7 @@ ll_status ll_start(ll_ctx *ctx, uint32_t offset) {
 
 static ll_status launch_iteration(ll_ctx *ctx, bool report) {
   launch_tall(ctx);
-  launch_wide(ctx, report ? WIDE_REPORT : WIDE_ITER);
+  launch_wide(ctx, report ? WIDE_REPORT : WIDE_ITER, true);
   CK(cudaGetLastError());
   ctx->offset = (uint32_t)((2ull * ctx->offset) % ctx->q);
   return LL_OK;
@@ -920,8 +966,8 @@ ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
       CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
       const uint32_t off0 = ctx->offset;
       for (uint32_t i = 0; i < K; ++i) {
-        launch_tall(ctx);
-        launch_wide(ctx, WIDE_ITER);
+        launch_tall(ctx, i > 0);
+        launch_wide(ctx, WIDE_ITER, true);
       }
       ctx->offset = off0;
       cudaError_t e = cudaStreamEndCapture(ctx->stream, &ctx->graph);
@@ -1364,8 +1410,8 @@ ll_status ll_batch_step(ll_batch *b, uint32_t iters, uint32_t flags, float *max_
         cudaStreamWaitEvent(c->stream, b->events[0], 0);
         const uint32_t off0 = c->offset;
         for (uint32_t k = 0; k < K; ++k) {
-          launch_tall(c);
-          launch_wide(c, WIDE_ITER);
+          launch_tall(c, k > 0);
+          launch_wide(c, WIDE_ITER, true);
         }
         c->offset = off0;
         cudaEventRecord(b->events[i + 1], c->stream);

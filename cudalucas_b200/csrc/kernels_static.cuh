@@ -99,26 +99,48 @@ __host__ __device__ constexpr bool palindromic() {
   return true;
 }
 
+// Shared-memory rows: element x of row `row` lives in slot row*RS + pad(x).
+// RS = L + L/16 for the tall pass (two columns, as one padded array); the
+// wide pass adds up to 7 slots per row so that the G rows of a CTA start
+// 8/G bank groups apart (its row-interleaved global loads and stores then
+// hit distinct banks).
+template <int L>
+__host__ __device__ constexpr int col_slots() { return L + L / 16; }
+template <int L, int G>
+__host__ __device__ constexpr int row_slots() {
+  return L + L / 16 + (G > 1 ? ((8 / G - (L + L / 16) % 8) % 8 + 8) % 8 : 0);
+}
+
 // One Stockham stage of every row of the CTA, in place in shared memory.
 // Thread t of a row handles butterflies t, t+TR, ... (a guard skips the
 // tail when L/R is not a multiple of TR).  `tw` points at this stage's
 // twiddle block (NS rows of R-1 entries) in shared memory.
-template <int L, int R, int NS, int SIGN, int TR>
+template <int L, int RS, int R, int NS, int SIGN, int TR>
 __device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, int t) {
+  const int rb = row * RS;
   constexpr int M = L / R;
   constexpr int NB = (M + TR - 1) / TR;
+  // When TR is a multiple of NS, every butterfly j = t + b*TR of this thread
+  // has the same twiddle row k = t mod NS: load it once (small radices only;
+  // for larger ones the registers it holds cost more than the loads).
+  constexpr bool kShared = NS > 1 && NB > 1 && TR % NS == 0 && R <= 8;
+  double2 wk[kShared ? R - 1 : 1];
+  if constexpr (kShared) {
+#pragma unroll
+    for (int r = 1; r < R; ++r) wk[r - 1] = tw[(t % NS) * tw_stride(R) + r - 1];
+  }
   double2 v[NB][R];
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const int j = t + b * TR;
     if (M % TR == 0 || j < M) {
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[b][r] = s[pad(row * L + j + r * M)];
+      for (int r = 0; r < R; ++r) v[b][r] = s[rb + pad(j + r * M)];
       if constexpr (NS > 1) {
         const int k = j % NS;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          const double2 w = tw[k * tw_stride(R) + r - 1];
+          const double2 w = kShared ? wk[r - 1] : tw[k * tw_stride(R) + r - 1];
           v[b][r] = SIGN > 0 ? cmul(v[b][r], w) : cmulc(v[b][r], w);
         }
       }
@@ -131,50 +153,50 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, i
     const int j = t + b * TR;
     if (M % TR == 0 || j < M) {
       const int k = j % NS;
-      const int ob = row * L + (j - k) * R + k;
+      const int ob = (j - k) * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) s[pad(ob + r * NS)] = v[b][sslot<R>(r)];
+      for (int r = 0; r < R; ++r) s[rb + pad(ob + r * NS)] = v[b][sslot<R>(r)];
     }
   }
   __syncthreads();
 }
 
 // forward stages [I, E) (radix a[I], NS = a[0]*...*a[I-1])
-template <class P, int I, int E, int NS, int TR>
+template <class P, int RS, int I, int E, int NS, int TR>
 __device__ __forceinline__ void fwd_stages(double2 *s, const double2 *tw, int row, int t) {
   if constexpr (I < E) {
     constexpr int R = P::a[I];
-    sstage<P::L, R, NS, +1, TR>(s, tw + tw_offset<P, I>(), row, t);
-    fwd_stages<P, I + 1, E, NS * R, TR>(s, tw, row, t);
+    sstage<P::L, RS, R, NS, +1, TR>(s, tw + tw_offset<P, I>(), row, t);
+    fwd_stages<P, RS, I + 1, E, NS * R, TR>(s, tw, row, t);
   }
 }
 
 // inverse stages [I, E) of the reversed list (radix a[N-1-I])
-template <class P, int I, int E, int NS, int TR>
+template <class P, int RS, int I, int E, int NS, int TR>
 __device__ __forceinline__ void inv_stages(double2 *s, const double2 *tw, int row, int t) {
   static_assert(palindromic<P>(), "inverse stages reuse the forward twiddle table");
   if constexpr (I < E) {
     constexpr int R = P::a[P::N - 1 - I];
-    sstage<P::L, R, NS, -1, TR>(s, tw + tw_offset<P, I>(), row, t);
-    inv_stages<P, I + 1, E, NS * R, TR>(s, tw, row, t);
+    sstage<P::L, RS, R, NS, -1, TR>(s, tw + tw_offset<P, I>(), row, t);
+    inv_stages<P, RS, I + 1, E, NS * R, TR>(s, tw, row, t);
   }
 }
 
 // Forward first stage (radix 16, no twiddle) from registers x[t + r*TR].
-template <int L, int TR>
+template <int L, int RS, int TR>
 __device__ __forceinline__ void first_stage_from_regs(double2 *s, double2 *v, int row, int t) {
   dft<16, +1>(v);
 #pragma unroll
-  for (int r = 0; r < 16; ++r) s[pad(row * L + t * 16 + r)] = v[out_slot<16>(r)];
+  for (int r = 0; r < 16; ++r) s[row * RS + pad(t * 16 + r)] = v[out_slot<16>(r)];
 }
 
 // Inverse last stage (radix 16, NS = L/16): leaves X[t + r*TR] in o[r].
 // tw is the stage's twiddle block (k = t, 15 entries per k).
-template <int L, int TR>
+template <int L, int RS, int TR>
 __device__ __forceinline__ void last_stage_to_regs(const double2 *s, const double2 *tw, double2 *o, int row, int t) {
   double2 v[16];
 #pragma unroll
-  for (int r = 0; r < 16; ++r) v[r] = s[pad(row * L + t + r * TR)];
+  for (int r = 0; r < 16; ++r) v[r] = s[row * RS + pad(t + r * TR)];
 #pragma unroll
   for (int r = 1; r < 16; ++r) v[r] = cmulc(v[r], tw[t * 15 + r - 1]);
   dft<16, -1>(v);
@@ -201,6 +223,17 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
 }
 
+// Programmatic dependent launch.  The passes are launched with programmatic
+// stream serialization, so a kernel may become resident while the previous
+// pass drains and run its prologue (tables, twiddles, ticket) early.
+// griddep_wait() returns once the previous kernel in the stream has completed
+// and its writes are visible; every read of the state array and of the device
+// state comes after it.  griddep_release() lets the next kernel start
+// launching; it is called only after griddep_wait(), so two launches of the
+// same pass never overlap.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <class P>
 __host__ __device__ constexpr int tall_extra() { return tw_size<P>() + 32 + 8; }
 
@@ -223,10 +256,6 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
   const int kB = special ? W / 2 : W - c;
   const int col = threadIdx.x / TR, t = threadIdx.x - col * TR;
   const int k1 = col ? kB : kA;
-  if (c == 0 && threadIdx.x == 0) {
-    const uint32_t o = a.st->offset;  // CUDALucas.cu:1882, once per iteration
-    a.st->offset = (uint32_t)((2ull * o) % a.q);
-  }
   for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
   if (threadIdx.x < 32) {
     const int kk = threadIdx.x < 16 ? kA : kB, r = threadIdx.x & 15;
@@ -235,6 +264,12 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
     pj[threadIdx.x - 32] = __ldg(&a.twH[(threadIdx.x - 32) * T]);
   }
   const double2 base = omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * t);
+  griddep_wait();
+  griddep_release();
+  if (c == 0 && threadIdx.x == 0) {
+    const uint32_t o = a.st->offset;  // CUDALucas.cu:1882, once per iteration
+    a.st->offset = (uint32_t)((2ull * o) % a.q);
+  }
   const double2 *src = a.A + (size_t)k1 * H;
   {
     double2 v[16];
@@ -244,10 +279,10 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = cmul(v[r], cmul(base, wr[col * 16 + r]));
-    first_stage_from_regs<H, TR>(sm, v, col, t);
+    first_stage_from_regs<H, col_slots<H>(), TR>(sm, v, col, t);
   }
   __syncthreads();
-  fwd_stages<P, 1, P::N, 16, TR>(sm, stw, col, t);
+  fwd_stages<P, col_slots<H>(), 1, P::N, 16, TR>(sm, stw, col, t);
   // pairing: loop index i = threadIdx.x + j*T, w_H^i = w_H^threadIdx.x * pj[j]
   const double2 wt = __ldg(&a.twH[threadIdx.x]);
   if (!special) {
@@ -288,9 +323,9 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
     }
   }
   __syncthreads();
-  inv_stages<P, 0, P::N - 1, 1, TR>(sm, stw, col, t);
+  inv_stages<P, col_slots<H>(), 0, P::N - 1, 1, TR>(sm, stw, col, t);
   double2 o[16];
-  last_stage_to_regs<H, TR>(sm, stw + tw_offset<P, P::N - 1>(), o, col, t);
+  last_stage_to_regs<H, col_slots<H>(), TR>(sm, stw + tw_offset<P, P::N - 1>(), o, col, t);
   double2 *dst = a.A + (size_t)k1 * H;
 #pragma unroll
   for (int r = 0; r < 16; ++r) dst[t + r * TR] = cmulc(o[r], cmul(base, wr[col * 16 + r]));
@@ -299,23 +334,26 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
 template <class P, int G>
 constexpr int wide_threads() { return G * (P::L / 16); }
 
-// Splits an integer-valued double v (|v| < 2^52) as v = h*2^b + l, 0 <= l < 2^b
-// (exact: scaling by powers of two and floor are exact in FP64).
-__device__ __forceinline__ void split_word(double v, double p2b, double ip2b, double &h, double &l) {
-  h = floor(v * ip2b);
-  l = fma(-h, p2b, v);
+// Nearest integer of x for |x| < 2^51 (ties to even) by adding and removing
+// 1.5*2^52: two FP64 adds instead of a rounding instruction.  The _rn
+// intrinsics are never contracted or reassociated.  The carry splits below
+// apply it to values below 2^37 in magnitude.
+__device__ __forceinline__ double rnd_int(double x) {
+  return __dsub_rn(__dadd_rn(x, 6755399441055744.0), 6755399441055744.0);
 }
 
 // Wide pass for rows of length W = P::L; G rows per CTA.
 // The carry arithmetic runs in FP64 on integer-valued doubles (all values
-// stay below 2^53, so every step is exact); carries are handed over as
-// int32 pairs (c1, c2).
+// stay below 2^53 and every scaling is by a power of two, so every step is
+// exact); carries are handed over as doubles, through shared memory between
+// the rows of a CTA and through global memory from CTA to CTA.
 template <class P, int G, int MODE>
 __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<P, G>())) wide_static(WideArgs a) {
   constexpr int W = P::L, TR = W / 16, T = G * TR;
   static_assert(P::a[0] == 16, "first radix must be 16");
   extern __shared__ double2 sm[];
-  double2 *stw = sm + padded(G * W);
+  constexpr int RS = row_slots<W, G>();
+  double2 *stw = sm + G * RS;
   __shared__ int s_g;
   __shared__ float s_err[32];
   __shared__ uint32_t s_fault;
@@ -329,11 +367,6 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   const int g = s_g;
   const int H = a.H;
   const int m2b = g * G;
-  if (MODE != WIDE_INIT)
-    for (int idx = threadIdx.x; idx < G * W; idx += T) {
-      const int k1 = idx / G, r = idx - k1 * G;
-      cp_async16(&sm[pad(r * W + k1)], &a.A[(size_t)k1 * H + m2b + r]);
-    }
   const int row = threadIdx.x / TR, t = threadIdx.x - row * TR;
   const int m2 = m2b + row;
   const int n = (int)a.n, bb = (int)a.b, qn = (int)a.qn;
@@ -351,13 +384,21 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   const double ip2lo = 1.0 / p2lo, ip2hi = 0.5 * ip2lo;
   double2 x[16];
   double emax = 0.0;
-  uint32_t fault = 0;
-
+  double Wi0 = 0.0, Wi1 = 0.0;
   if (MODE != WIDE_INIT) {
     const double cwit = __ldg(&a.colWi[t]);
-    const double Wi0 = __ldg(&a.rowWi[2 * m2]) * cwit * (__ldg(&a.rowE[2 * m2]) + __ldg(&a.colF[t]) >= n ? 2.0 : 1.0);
-    const double Wi1 =
-        __ldg(&a.rowWi[2 * m2 + 1]) * cwit * (__ldg(&a.rowE[2 * m2 + 1]) + __ldg(&a.colF[t]) >= n ? 2.0 : 1.0);
+    Wi0 = __ldg(&a.rowWi[2 * m2]) * cwit * (__ldg(&a.rowE[2 * m2]) + __ldg(&a.colF[t]) >= n ? 2.0 : 1.0);
+    Wi1 = __ldg(&a.rowWi[2 * m2 + 1]) * cwit * (__ldg(&a.rowE[2 * m2 + 1]) + __ldg(&a.colF[t]) >= n ? 2.0 : 1.0);
+  }
+  // everything above reads constant tables only; the state array, the
+  // digits and the device state are read after the previous pass completed
+  griddep_wait();
+  griddep_release();
+  if (MODE != WIDE_INIT) {
+    for (int idx = threadIdx.x; idx < G * W; idx += T) {
+      const int k1 = idx / G, r = idx - k1 * G;
+      cp_async16(&sm[r * RS + pad(k1)], &a.A[(size_t)k1 * H + m2b + r]);
+    }
     // the -2 (bit (offset+1) mod q, CUDALucas.cu:1882-1886) hits at most one
     // word; locate it once: element register r_sub, word w_sub
     const uint32_t off = a.st->offset;
@@ -373,15 +414,17 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
     const bool w_sub = dw & 1;
     cp_async_wait_all();
     __syncthreads();
-    inv_stages<P, 0, P::N - 1, 1, TR>(sm, stw, row, t);
+    inv_stages<P, RS, 0, P::N - 1, 1, TR>(sm, stw, row, t);
     double2 u[16];
-    last_stage_to_regs<W, TR>(sm, stw + tw_offset<P, P::N - 1>(), u, row, t);
+    last_stage_to_regs<W, RS, TR>(sm, stw + tw_offset<P, P::N - 1>(), u, row, t);
     __syncthreads();  // shared memory is reused for the carry hand-off below
 
-    int2 *cs = reinterpret_cast<int2 *>(sm);
-    int2 *gc = reinterpret_cast<int2 *>(a.carry);
-    // kept across the hand-off: low part of word 0 and balanced word 1
-    int2 keep[16];
+    // Carry in FP64 only (no integer conversions).  Phase 1 leaves, in the
+    // shared-memory slot of element (row, m1), the packed pair
+    // l0 + d1p*2^24 (|l0|, |d1p| <= 2^(bits-1) < 2^23, so the pair is exact
+    // and separable) and the element's outgoing carry.
+    double2 *ks = sm + row * W + t;  // ks[r*TR]: element m1 = t + r*TR
+    double *gcd = reinterpret_cast<double *>(a.carry);
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
@@ -397,22 +440,23 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
         else r0 -= sub;
       }
       const bool big0 = e0 < bb, big1 = e1 < bb;
+      const double P0 = big0 ? p2hi : p2lo, I0 = big0 ? ip2hi : ip2lo;
       const double P1 = big1 ? p2hi : p2lo, I1 = big1 ? ip2hi : ip2lo;
-      // word i keeps bal(low_i + c1_{i-1}) + c2_{i-1}: c1 is the high part of
-      // the previous word, c2 the carry out of balancing the previous word
-      double h0, l0, h1, l1;
-      split_word(r0, big0 ? p2hi : p2lo, big0 ? ip2hi : ip2lo, h0, l0);
-      split_word(r1, P1, I1, h1, l1);
+      // balanced splits r = h*2^bits + l; word 1 takes high_0 and is
+      // balanced again; the outgoing carry high_1 + (carry of that balance)
+      // depends on this element's own words only
+      const double h0 = rnd_int(r0 * I0), l0 = fma(-h0, P0, r0);
+      const double h1 = rnd_int(r1 * I1), l1 = fma(-h1, P1, r1);
       const double tt1 = l1 + h0;
-      const double k1c = floor((tt1 + 0.5 * P1) * I1);
+      const double k1c = rnd_int(tt1 * I1);
       const double d1p = fma(-k1c, P1, tt1);
-      if (fabs(h1) >= 2147483647.0 || fabs(k1c) >= 2147483647.0) fault |= 2u;
-      keep[r] = make_int2((int)l0, (int)d1p);
-      const int2 pc = make_int2((int)h1, (int)k1c);  // outgoing (c1, c2)
-      cs[row * W + m1] = pc;
-      if (row == G - 1) gc[(size_t)g * W + m1] = pc;
+      const double co = h1 + k1c;
+      ks[r * TR] = make_double2(fma(d1p, 0x1p24, l0), co);
+      if (row == G - 1) gcd[(size_t)g * W + m1] = co;
     }
-    if (row == G - 1) __threadfence();
+    // the release store of the ready flag below (after the barrier) orders
+    // the carry stores of all threads before the flag for the successor's
+    // acquire
     __syncthreads();
     const int pred = g == 0 ? a.ngroups - 1 : g - 1;
     if (threadIdx.x == 0) {
@@ -424,21 +468,19 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
-      int2 cin;
-      if (row > 0) cin = cs[(row - 1) * W + m1];
-      else {
-        const long long raw = __ldcg(&a.carry[(size_t)pred * W + (g == 0 ? (m1 == 0 ? W - 1 : m1 - 1) : m1)]);
-        cin = make_int2((int)(raw & 0xffffffffll), (int)(raw >> 32));
-      }
+      const double cin = row > 0 ? sm[(row - 1) * W + m1].y
+                                 : __ldcg(&gcd[(size_t)pred * W + (g == 0 ? (m1 == 0 ? W - 1 : m1 - 1) : m1)]);
       const int D = a.colD[r];
       const bool n0 = E0 < D, n1 = E1 < D;
       const int e0 = E0 - D + (n0 ? n : 0);
       const bool big0 = e0 < bb;
       const double P0 = big0 ? p2hi : p2lo, I0 = big0 ? ip2hi : ip2lo;
-      const double tt0 = (double)keep[r].x + (double)cin.x;
-      const double k0 = floor((tt0 + 0.5 * P0) * I0);
-      const double d0 = fma(-k0, P0, tt0) + (double)cin.y;
-      const double d1 = (double)keep[r].y + k0;
+      const double pk = ks[r * TR].x;
+      const double d1p = rnd_int(pk * 0x1p-24), l0 = fma(-d1p, 0x1p24, pk);
+      const double tt0 = l0 + cin;
+      const double k0 = rnd_int(tt0 * I0);
+      const double d0 = fma(-k0, P0, tt0);
+      const double d1 = d1p + k0;
       if (MODE == WIDE_REPORT) {
         const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
         a.xint[j0] = (int32_t)d0;
@@ -460,19 +502,18 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
                           (double)a.xint[j0 + 1] * (W1 * (n1 ? a.colS2[r] : a.colS[r])));
     }
   }
-  first_stage_from_regs<W, TR>(sm, x, row, t);
+  first_stage_from_regs<W, RS, TR>(sm, x, row, t);
   __syncthreads();
-  fwd_stages<P, 1, P::N, 16, TR>(sm, stw, row, t);
+  fwd_stages<P, RS, 1, P::N, 16, TR>(sm, stw, row, t);
   for (int idx = threadIdx.x; idx < G * W; idx += T) {
     const int k1 = idx / G, r = idx - k1 * G;
-    a.A[(size_t)k1 * H + m2b + r] = sm[pad(r * W + k1)];
+    a.A[(size_t)k1 * H + m2b + r] = sm[r * RS + pad(k1)];
   }
   if (MODE != WIDE_INIT) {
-#pragma unroll
     float em = (float)emax;
+#pragma unroll
     for (int o = 16; o; o >>= 1) em = fmaxf(em, __shfl_xor_sync(0xffffffffu, em, o));
     if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = em;
-    if (fault) atomicOr(&s_fault, fault);
     __syncthreads();
     if (threadIdx.x == 0) {
       float m = 0.f;
