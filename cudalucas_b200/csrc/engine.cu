@@ -377,7 +377,8 @@ struct StaticTall {
   int L;
   void (*run)(TallArgs);
   int nrad, rad[4];
-  int extra;
+  int extra;  // shared-memory entries beyond the two columns
+  int tw;     // of which stage twiddles (the first entries)
 };
 
 #define LLB_WIDE(LIST, G)                                                                                       \
@@ -385,7 +386,8 @@ struct StaticTall {
    LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tw_size<LIST>(),             \
    G * row_slots<LIST::L, G>()}
 #define LLB_TALL(LIST) \
-  {LIST::L, tall_static<LIST>, LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tall_extra<LIST>()}
+  {LIST::L, tall_static<LIST>, LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, \
+   tall_extra<LIST>(), tw_size<LIST>()}
 
 using L512 = RList<16, 2, 16>;
 using L768 = RList<16, 3, 16>;
@@ -714,7 +716,7 @@ static ll_status build_tables(ll_ctx *ctx) {
   }
   if (ctx->shape.st) {
     std::vector<double2> t = stage_twiddles(ctx->shape.st->rad, ctx->shape.st->nrad);
-    if ((int)t.size() + 40 != ctx->shape.st->extra) return LL_ERR_SHAPE;
+    if ((int)t.size() != ctx->shape.st->tw) return LL_ERR_SHAPE;
     CK(upload(&ctx->stwH, t));
   }
   CK(upload(&ctx->rowE, rE));
@@ -1173,7 +1175,7 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
   int32_t *h_cF = (int32_t *)hput(sizeof(int32_t) * W);
   double *h_cW = (double *)hput(sizeof(double) * W);
   double *h_cWi = (double *)hput(sizeof(double) * W);
-  const size_t n_stwW = s.sw ? (size_t)s.sw->extra : 0, n_stwH = s.st ? (size_t)(s.st->extra - 40) : 0;
+  const size_t n_stwW = s.sw ? (size_t)s.sw->extra : 0, n_stwH = s.st ? (size_t)s.st->tw : 0;
   double2 *h_stwW = (double2 *)hput(sizeof(double2) * (n_stwW ? n_stwW : 1));
   double2 *h_stwH = (double2 *)hput(sizeof(double2) * (n_stwH ? n_stwH : 1));
   if (!h_stwH) return LL_ERR_ARG;

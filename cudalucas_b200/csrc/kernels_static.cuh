@@ -127,7 +127,7 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, i
   double2 wk[kShared ? R - 1 : 1];
   if constexpr (kShared) {
 #pragma unroll
-    for (int r = 1; r < R; ++r) wk[r - 1] = tw[(t % NS) * tw_stride(R) + r - 1];
+    for (int r = 1; r < R; ++r) wk[r - 1] = tw[(int)((unsigned)t % NS) * tw_stride(R) + r - 1];
   }
   double2 v[NB][R];
 #pragma unroll
@@ -137,7 +137,7 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, i
 #pragma unroll
       for (int r = 0; r < R; ++r) v[b][r] = s[rb + pad(j + r * M)];
       if constexpr (NS > 1) {
-        const int k = j % NS;
+        const int k = (int)((unsigned)j % NS);
 #pragma unroll
         for (int r = 1; r < R; ++r) {
           const double2 w = kShared ? wk[r - 1] : tw[k * tw_stride(R) + r - 1];
@@ -152,7 +152,7 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, i
   for (int b = 0; b < NB; ++b) {
     const int j = t + b * TR;
     if (M % TR == 0 || j < M) {
-      const int k = j % NS;
+      const int k = (int)((unsigned)j % NS);
       const int ob = (j - k) * R + k;
 #pragma unroll
       for (int r = 0; r < R; ++r) s[rb + pad(ob + r * NS)] = v[b][sslot<R>(r)];
@@ -182,24 +182,27 @@ __device__ __forceinline__ void inv_stages(double2 *s, const double2 *tw, int ro
   }
 }
 
-// Forward first stage (radix 16, no twiddle) from registers x[t + r*TR].
-template <int L, int RS, int TR>
+// First stage (radix 16, no twiddle) from registers x[t + r*TR]: of the
+// forward transform (SIGN +1), or of the inverse one (SIGN -1, the reversed
+// list starts with the same radix 16).
+template <int L, int RS, int TR, int SIGN = +1>
 __device__ __forceinline__ void first_stage_from_regs(double2 *s, double2 *v, int row, int t) {
-  dft<16, +1>(v);
+  dft<16, SIGN>(v);
 #pragma unroll
   for (int r = 0; r < 16; ++r) s[row * RS + pad(t * 16 + r)] = v[out_slot<16>(r)];
 }
 
-// Inverse last stage (radix 16, NS = L/16): leaves X[t + r*TR] in o[r].
-// tw is the stage's twiddle block (k = t, 15 entries per k).
-template <int L, int RS, int TR>
+// Last stage (radix 16, NS = L/16) into registers: leaves X[t + r*TR] in
+// o[r].  tw is the stage's twiddle block (k = t, 15 entries per k); SIGN -1
+// for the inverse transform, +1 for the forward one.
+template <int L, int RS, int TR, int SIGN = -1>
 __device__ __forceinline__ void last_stage_to_regs(const double2 *s, const double2 *tw, double2 *o, int row, int t) {
   double2 v[16];
 #pragma unroll
   for (int r = 0; r < 16; ++r) v[r] = s[row * RS + pad(t + r * TR)];
 #pragma unroll
-  for (int r = 1; r < 16; ++r) v[r] = cmulc(v[r], tw[t * 15 + r - 1]);
-  dft<16, -1>(v);
+  for (int r = 1; r < 16; ++r) v[r] = SIGN > 0 ? cmul(v[r], tw[t * 15 + r - 1]) : cmulc(v[r], tw[t * 15 + r - 1]);
+  dft<16, SIGN>(v);
 #pragma unroll
   for (int r = 0; r < 16; ++r) o[r] = v[out_slot<16>(r)];
 }
@@ -367,7 +370,13 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   const int g = s_g;
   const int H = a.H;
   const int m2b = g * G;
-  const int row = threadIdx.x / TR, t = threadIdx.x - row * TR;
+  // The G rows of an element column m1 sit in adjacent lanes.  With G >= 2
+  // the global loads and stores of A[m1*H + m2b + row] then cover whole
+  // 32-byte sectors, so the edge stages of the row transforms read and write
+  // global memory directly; a single row (G = 1) touches half sectors, and
+  // is staged through shared memory with cp.async instead.
+  constexpr bool kDirect = G > 1;
+  const int row = threadIdx.x % G, t = threadIdx.x / G;
   const int m2 = m2b + row;
   const int n = (int)a.n, bb = (int)a.b, qn = (int)a.qn;
   // Word s (0, 1) of element (m1 = t + r*TR, m2) has weight exponent
@@ -395,9 +404,16 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   griddep_wait();
   griddep_release();
   if (MODE != WIDE_INIT) {
-    for (int idx = threadIdx.x; idx < G * W; idx += T) {
-      const int k1 = idx / G, r = idx - k1 * G;
-      cp_async16(&sm[r * RS + pad(k1)], &a.A[(size_t)k1 * H + m2b + r]);
+    if constexpr (kDirect) {
+      // the inverse transform's first stage (radix 16, no twiddle) works on
+      // elements t + r*TR of the row: straight from global memory
+      double2 v[16];
+      const double2 *src = a.A + m2;
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = src[(size_t)(t + r * TR) * H];
+      first_stage_from_regs<W, RS, TR, -1>(sm, v, row, t);
+    } else {
+      for (int k1 = threadIdx.x; k1 < W; k1 += T) cp_async16(&sm[pad(k1)], &a.A[(size_t)k1 * H + m2b]);
     }
     // the -2 (bit (offset+1) mod q, CUDALucas.cu:1882-1886) hits at most one
     // word; locate it once: element register r_sub, word w_sub
@@ -414,7 +430,8 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
     const bool w_sub = dw & 1;
     cp_async_wait_all();
     __syncthreads();
-    inv_stages<P, RS, 0, P::N - 1, 1, TR>(sm, stw, row, t);
+    if constexpr (kDirect) inv_stages<P, RS, 1, P::N - 1, 16, TR>(sm, stw, row, t);
+    else inv_stages<P, RS, 0, P::N - 1, 1, TR>(sm, stw, row, t);
     double2 u[16];
     last_stage_to_regs<W, RS, TR>(sm, stw + tw_offset<P, P::N - 1>(), u, row, t);
     __syncthreads();  // shared memory is reused for the carry hand-off below
@@ -423,7 +440,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
     // shared-memory slot of element (row, m1), the packed pair
     // l0 + d1p*2^24 (|l0|, |d1p| <= 2^(bits-1) < 2^23, so the pair is exact
     // and separable) and the element's outgoing carry.
-    double2 *ks = sm + row * W + t;  // ks[r*TR]: element m1 = t + r*TR
+    double2 *ks = sm + row * RS + t;  // ks[r*TR]: element m1 = t + r*TR
     double *gcd = reinterpret_cast<double *>(a.carry);
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
@@ -468,7 +485,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
-      const double cin = row > 0 ? sm[(row - 1) * W + m1].y
+      const double cin = row > 0 ? sm[(row - 1) * RS + m1].y
                                  : __ldcg(&gcd[(size_t)pred * W + (g == 0 ? (m1 == 0 ? W - 1 : m1 - 1) : m1)]);
       const int D = a.colD[r];
       const bool n0 = E0 < D, n1 = E1 < D;
@@ -504,10 +521,17 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   }
   first_stage_from_regs<W, RS, TR>(sm, x, row, t);
   __syncthreads();
-  fwd_stages<P, RS, 1, P::N, 16, TR>(sm, stw, row, t);
-  for (int idx = threadIdx.x; idx < G * W; idx += T) {
-    const int k1 = idx / G, r = idx - k1 * G;
-    a.A[(size_t)k1 * H + m2b + r] = sm[r * RS + pad(k1)];
+  if constexpr (kDirect) {
+    fwd_stages<P, RS, 1, P::N - 1, 16, TR>(sm, stw, row, t);
+    // the last stage (radix 16) leaves elements t + r*TR in registers: store
+    // them straight to global memory
+    last_stage_to_regs<W, RS, TR, +1>(sm, stw + tw_offset<P, P::N - 1>(), x, row, t);
+    double2 *dst = a.A + m2;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) dst[(size_t)(t + r * TR) * H] = x[r];
+  } else {
+    fwd_stages<P, RS, 1, P::N, 16, TR>(sm, stw, row, t);
+    for (int k1 = threadIdx.x; k1 < W; k1 += T) a.A[(size_t)k1 * H + m2b] = sm[pad(k1)];
   }
   if (MODE != WIDE_INIT) {
     float em = (float)emax;
