@@ -73,12 +73,16 @@ struct TallArgs {
   uint32_t q;
 };
 
+// Ready flags per wide-pass CTA: the specialised kernels hand the carry over
+// warp by warp (at most 16 warps per CTA); the generic ones use the first.
+constexpr int kWarpFlags = 16;
+
 struct WideArgs {
   double2 *A;
   const double2 *stw;   // stage twiddles of the specialised row transform
   int32_t *xint;
   long long *carry;     // packed carries, one row of W per CTA
-  uint32_t *flags;      // one ready flag per CTA
+  uint32_t *flags;      // ready flags: kWarpFlags per CTA (one per warp)
   const double2 *twW;
   const int32_t *rowE;  // ((-(2*m2+t)*b) mod n), 2H entries
   const double *rowW;   // 2^(rowE/n)
@@ -775,12 +779,12 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
     if ((e = cudaMalloc((void **)&ctx->A, sizeof(double2) * (size_t)ctx->N)) != cudaSuccess ||
         (e = cudaMalloc((void **)&ctx->xint, sizeof(int32_t) * (size_t)n)) != cudaSuccess ||
         (e = cudaMalloc((void **)&ctx->carry, sizeof(long long) * (size_t)ngroups * s.W)) != cudaSuccess ||
-        (e = cudaMalloc((void **)&ctx->flags, sizeof(uint32_t) * (size_t)ngroups)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&ctx->flags, sizeof(uint32_t) * kWarpFlags * (size_t)ngroups)) != cudaSuccess ||
         (e = cudaMalloc((void **)&ctx->st, sizeof(DevState))) != cudaSuccess) {
       rc = e == cudaErrorMemoryAllocation ? LL_ERR_NOMEM : cuda_fail(ctx, e, "cudaMalloc");
       break;
     }
-    if ((e = cudaMemset(ctx->flags, 0, sizeof(uint32_t) * (size_t)ngroups)) != cudaSuccess ||
+    if ((e = cudaMemset(ctx->flags, 0, sizeof(uint32_t) * kWarpFlags * (size_t)ngroups)) != cudaSuccess ||
         (e = cudaMemset(ctx->st, 0, sizeof(DevState))) != cudaSuccess) {
       rc = cuda_fail(ctx, e, "cudaMemset");
       break;
@@ -1227,7 +1231,7 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
   };
   double2 *A = (double2 *)dput(sizeof(double2) * (size_t)N);
   long long *carry = (long long *)dput(sizeof(long long) * (size_t)ngroups * W);
-  uint32_t *flags = (uint32_t *)dput(sizeof(uint32_t) * (size_t)ngroups);
+  uint32_t *flags = (uint32_t *)dput(sizeof(uint32_t) * kWarpFlags * (size_t)ngroups);
   DevState *dst = (DevState *)dput(sizeof(DevState));
   unsigned char *dtab = dput(table_bytes);
   if (o > kScratchBytes) return LL_ERR_ARG;  // shape needs more scratch than the static array holds
@@ -1278,7 +1282,7 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
   // ---- state that must start at zero: flags, ticket, error, fault
   DevState hs{};
   hs.offset = offset;
-  if ((e = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * (size_t)ngroups, st)) != cudaSuccess ||
+  if ((e = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * kWarpFlags * (size_t)ngroups, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(dst, &hs, sizeof(DevState), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(dtab, g_host_tables, table_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return LL_ERR_CUDA;

@@ -147,7 +147,9 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, i
       sdft<R, SIGN>(v[b]);
     }
   }
-  __syncthreads();
+  // with one butterfly per thread and NS == L/R a thread stores exactly the
+  // slots it loaded: no barrier between the loads and the stores
+  if constexpr (!(NB == 1 && NS == M)) __syncthreads();
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const int j = t + b * TR;
@@ -237,21 +239,45 @@ __device__ __forceinline__ void cp_async_wait_all() {
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void griddep_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Pairing strategy of the tall pass: when every warp holds threads of one
+// column only (TR a multiple of 32), each thread pairs its own bins with the
+// mirror bins of its partner thread in the other column (half exchange);
+// otherwise all bins go through shared memory and the pairs are split over
+// the CTA by index.
 template <class P>
-__host__ __device__ constexpr int tall_extra() { return tw_size<P>() + 32 + 8; }
+__host__ __device__ constexpr bool tall_half_exchange() { return (P::L / 16) % 32 == 0; }
 
-// Tall pass for columns of length H = P::L; two columns per CTA.
+template <class P>
+__host__ __device__ constexpr int tall_extra() {
+  return tw_size<P>() + 32 + 8 + (tall_half_exchange<P>() ? 16 + 4 * (P::L / 16) : 0);
+}
+
+// Tall pass for columns of length H = P::L (radix list 16, M, 16); two
+// columns per CTA.
 // The column twiddle w_N^(k1*m2) of element m2 = t + r*TR is formed as
 // w_N^(k1*t) (one table product per thread) times w_N^(k1*TR*r) (shared by
 // the CTA), so no per-element table gathers are needed.
+// The forward transform's last stage leaves bins t + r*TR (r < 16) of the
+// thread's column in its registers and in its own shared-memory slots; the
+// inverse transform's first stage reads exactly those slots.  Bin t + r*TR
+// of column kA pairs with bin H-1-(t + r*TR) = (TR-1-t) + (15-r)*TR of
+// column kB, which belongs to thread TR-1-t of the other column.  With the
+// half exchange each thread computes the pairs of its bins r < 8 (the
+// mirror bins, r >= 8 of the partner, come through shared memory) and writes
+// the partner's results back into the partner's slots.  (CTA 0 holds the
+// self-paired columns 0 and W/2 and always pairs through shared memory.)
 template <class P>
 __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>())) tall_static(TallArgs a) {
-  constexpr int H = P::L, TR = H / 16, T = 2 * TR;
-  static_assert(P::a[0] == 16, "first radix must be 16");
+  constexpr int H = P::L, TR = H / 16, T = 2 * TR, CS = col_slots<H>();
+  constexpr bool kHalf = tall_half_exchange<P>();
+  static_assert(P::N == 3 && P::a[0] == 16 && P::a[2] == 16, "radix list 16, M, 16");
   extern __shared__ double2 sm[];
   double2 *stw = sm + padded(2 * H);
-  double2 *wr = stw + tw_size<P>();
-  double2 *pj = wr + 32;
+  double2 *wr = stw + tw_size<P>();  // w_N^(k*TR*r), both columns
+  double2 *pj = wr + 32;             // w_H^(j*T), pairing by index
+  double2 *fr = pj + 8;              // w_H^(r*TR), half exchange
+  double2 *sbase = fr + 16;          // per thread: w_N^(k1*t), half exchange
+  double2 *spair = sbase + T;        // per thread: w_N^kA * w_H^tA, half exchange
   const int c = blockIdx.x;
   const int W = a.W;
   const bool special = (c == 0);
@@ -265,8 +291,17 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
     wr[threadIdx.x] = omegaN(a.thi, a.tlo, a.ts, a.tmask, kk * TR * r);
   } else if (threadIdx.x < 40) {
     pj[threadIdx.x - 32] = __ldg(&a.twH[(threadIdx.x - 32) * T]);
+  } else if (kHalf && threadIdx.x < 56) {
+    fr[threadIdx.x - 40] = __ldg(&a.twH[(threadIdx.x - 40) * TR]);
   }
-  const double2 base = omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * t);
+  // with the half exchange the per-thread twiddle bases are parked in the
+  // thread's own shared-memory slot while the transforms hold the registers
+  // (tA is the column-kA bin row of the thread's pairs)
+  double2 base = omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * t);
+  if constexpr (kHalf) {
+    sbase[threadIdx.x] = base;
+    spair[threadIdx.x] = cmul(omegaN(a.thi, a.tlo, a.ts, a.tmask, kA), __ldg(&a.twH[col ? TR - 1 - t : t]));
+  }
   griddep_wait();
   griddep_release();
   if (c == 0 && threadIdx.x == 0) {
@@ -280,56 +315,90 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
     for (int r = 0; r < 16; ++r) v[r] = src[t + r * TR];
     cp_async_wait_all();
     __syncthreads();
+    if constexpr (kHalf) base = sbase[threadIdx.x];
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = cmul(v[r], cmul(base, wr[col * 16 + r]));
-    first_stage_from_regs<H, col_slots<H>(), TR>(sm, v, col, t);
+    first_stage_from_regs<H, CS, TR>(sm, v, col, t);
   }
   __syncthreads();
-  fwd_stages<P, col_slots<H>(), 1, P::N, 16, TR>(sm, stw, col, t);
-  // pairing: loop index i = threadIdx.x + j*T, w_H^i = w_H^threadIdx.x * pj[j]
-  const double2 wt = __ldg(&a.twH[threadIdx.x]);
-  if (!special) {
-    const double2 wb = cmul(omegaN(a.thi, a.tlo, a.ts, a.tmask, kA), wt);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int k2 = threadIdx.x + j * T;
-      double2 za = sm[pad(k2)], zb = sm[pad(2 * H - 1 - k2)];
-      pair_square(za, zb, cmul(wb, pj[j]));
-      sm[pad(k2)] = za;
-      sm[pad(2 * H - 1 - k2)] = zb;
-    }
-  } else {
-    const int half = H / 2;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {  // column 0: k2 <-> (H-k2) mod H, w_N^(W*k2) = w_H^k2
-      const int i = threadIdx.x + j * T;
-      if (i <= half) {
-        const int p = (H - i) % H;
-        double2 za = sm[pad(i)], zb = sm[pad(p)];
-        pair_square(za, zb, cmul(wt, pj[j]));
-        sm[pad(i)] = za;
-        if (p != i) sm[pad(p)] = zb;
-      }
-    }
-    if (threadIdx.x == 0) {  // i = half + ... covered above only when half < 8*T
-    }
-    const double2 wb = cmul(omegaN(a.thi, a.tlo, a.ts, a.tmask, W / 2), wt);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {  // column W/2: k2 <-> H-1-k2
-      const int i = threadIdx.x + j * T;
-      if (i < half) {
-        double2 za = sm[pad(H + i)], zb = sm[pad(2 * H - 1 - i)];
-        pair_square(za, zb, cmul(wb, pj[j]));
-        sm[pad(H + i)] = za;
-        sm[pad(2 * H - 1 - i)] = zb;
-      }
-    }
-  }
-  __syncthreads();
-  inv_stages<P, col_slots<H>(), 0, P::N - 1, 1, TR>(sm, stw, col, t);
+  fwd_stages<P, CS, 1, P::N - 1, 16, TR>(sm, stw, col, t);
   double2 o[16];
-  last_stage_to_regs<H, col_slots<H>(), TR>(sm, stw + tw_offset<P, P::N - 1>(), o, col, t);
+  last_stage_to_regs<H, CS, TR, +1>(sm, stw + tw_offset<P, P::N - 1>(), o, col, t);
+  double2 *own = sm + col * CS;  // own bin r: own[pad(t + r*TR)]
+  if (kHalf && !special) {
+#pragma unroll
+    for (int r = 8; r < 16; ++r) own[pad(t + r * TR)] = o[r];
+    __syncthreads();
+    double2 *mir = sm + (col ^ 1) * CS;  // partner's bin 15-r: mir[pad(TR-1-t + (15-r)*TR)]
+    // Swapping the two bins and conjugating w swaps the two results of
+    // pair_square, so both columns make the same call: column kB passes its
+    // own bin first and conj(w).
+    const double2 wb = spair[threadIdx.x];
+    const double sg = col ? -1.0 : 1.0;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      const int ps = pad(TR - 1 - t + (15 - r) * TR);
+      double2 zm = mir[ps];
+      double2 w = cmul(wb, fr[col ? 15 - r : r]);
+      w.y *= sg;
+      pair_square(o[r], zm, w);
+      mir[ps] = zm;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 8; r < 16; ++r) o[r] = own[pad(t + r * TR)];
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) own[pad(t + r * TR)] = o[r];
+    __syncthreads();
+    // pairing by index: i = threadIdx.x + j*T, w_H^i = w_H^threadIdx.x * pj[j]
+    const double2 wt = __ldg(&a.twH[threadIdx.x]);
+    if (!special) {
+      const double2 wb = cmul(omegaN(a.thi, a.tlo, a.ts, a.tmask, kA), wt);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {  // bin k2 of column kA <-> bin H-1-k2 of column kB
+        const int k2 = threadIdx.x + j * T;
+        double2 za = sm[pad(k2)], zb = sm[pad(2 * H - 1 - k2)];
+        pair_square(za, zb, cmul(wb, pj[j]));
+        sm[pad(k2)] = za;
+        sm[pad(2 * H - 1 - k2)] = zb;
+      }
+    } else {
+      const int half = H / 2;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {  // column 0: k2 <-> (H-k2) mod H, w_N^(W*k2) = w_H^k2
+        const int i = threadIdx.x + j * T;
+        if (i <= half) {
+          const int p = (H - i) % H;
+          double2 za = sm[pad(i)], zb = sm[pad(p)];
+          pair_square(za, zb, cmul(wt, pj[j]));
+          sm[pad(i)] = za;
+          if (p != i) sm[pad(p)] = zb;
+        }
+      }
+      const double2 wb = cmul(omegaN(a.thi, a.tlo, a.ts, a.tmask, W / 2), wt);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {  // column W/2: k2 <-> H-1-k2
+        const int i = threadIdx.x + j * T;
+        if (i < half) {
+          double2 za = sm[pad(H + i)], zb = sm[pad(2 * H - 1 - i)];
+          pair_square(za, zb, cmul(wb, pj[j]));
+          sm[pad(H + i)] = za;
+          sm[pad(2 * H - 1 - i)] = zb;
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 16; ++r) o[r] = own[pad(t + r * TR)];
+  }
+  __syncthreads();  // every thread's slot reads are done before the stage-0 stores
+  first_stage_from_regs<H, CS, TR, -1>(sm, o, col, t);
+  __syncthreads();
+  inv_stages<P, CS, 1, P::N - 1, 16, TR>(sm, stw, col, t);
+  last_stage_to_regs<H, CS, TR>(sm, stw + tw_offset<P, P::N - 1>(), o, col, t);
   double2 *dst = a.A + (size_t)k1 * H;
+  if constexpr (kHalf) base = sbase[threadIdx.x];
 #pragma unroll
   for (int r = 0; r < 16; ++r) dst[t + r * TR] = cmulc(o[r], cmul(base, wr[col * 16 + r]));
 }
@@ -471,17 +540,37 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
       ks[r * TR] = make_double2(fma(d1p, 0x1p24, l0), co);
       if (row == G - 1) gcd[(size_t)g * W + m1] = co;
     }
-    // the release store of the ready flag below (after the barrier) orders
-    // the carry stores of all threads before the flag for the successor's
-    // acquire
-    __syncthreads();
+    // Hand-off warp by warp: warp w holds the same element columns m1 in
+    // every CTA, so it publishes its last row's carries with its own flag
+    // and waits only for the flag of warp w of the predecessor.  __syncwarp
+    // orders the lanes' stores and loads around lane 0's release store and
+    // acquire load.  (The wrap into CTA 0 shifts m1 by one across warps, so
+    // CTA 0 waits for all warps of the last CTA.)
     const int pred = g == 0 ? a.ngroups - 1 : g - 1;
-    if (threadIdx.x == 0) {
-      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&a.flags[g]), "r"(1u) : "memory");
-      if (!wait_flag(&a.flags[pred])) s_fault |= 1u;
-      a.flags[pred] = 0;
+    constexpr int NW = T / 32;
+    static_assert(T % 32 == 0 && NW <= kWarpFlags, "whole warps, one flag each");
+    const int warp = threadIdx.x >> 5;
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0)
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&a.flags[g * kWarpFlags + warp]), "r"(1u) : "memory");
+    if (g != 0) {
+      if ((threadIdx.x & 31) == 0) {
+        uint32_t *f = &a.flags[pred * kWarpFlags + warp];
+        if (!wait_flag(f)) atomicOr(&s_fault, 1u);
+        *f = 0;
+      }
+      __syncwarp();
+    } else {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        for (int w = 0; w < NW; ++w) {
+          uint32_t *f = &a.flags[pred * kWarpFlags + w];
+          if (!wait_flag(f)) s_fault |= 1u;
+          *f = 0;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
