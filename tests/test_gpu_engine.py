@@ -145,6 +145,37 @@ def test_c3_18432k_matches_exact_and_reference_binary():
             assert c.res64() == checks[k]
 
 
+@pytest.mark.parametrize("q,n,widths", [
+    # N = 1024*1024: specialised rows of 512 (4 per CTA), 1024 and 2048 (2 per
+    # CTA), columns with half-exchange pairing, and the generic kernels
+    (36700049, 2097152, [512, 1024, 2048, None]),
+    # N = 1280*768: columns of 768 and 1280 (threads of both columns in one
+    # warp), rows of 1280 and 768
+    (34603069, 1966080, [768, 1280, None]),
+])
+def test_kernel_variants_agree(q, n, widths):
+    """Every launch shape of one length (specialised kernels for several row
+    and column lengths, and the generic kernels) gives the oracle's residue
+    after a few iterations and the same residue after many."""
+    off = q // 3
+    o = Oracle(q, n)
+    o.start(off)
+    o.step(8)
+    want8 = o.res64()
+    got8, got300 = {}, {}
+    for w in widths:
+        tuning = {"width": w} if w else {"width": 1024, "rows_per_cta": 2}
+        with cl.LLContext(q, n, tuning=tuning) as c:
+            c.start(off)
+            e1 = c.step(8, report=True)
+            got8[w] = c.res64()
+            e2 = c.step(292, report=True)
+            got300[w] = c.res64()
+            assert max(e1, e2) < 0.4, (w, e1, e2)
+    assert all(v == want8 for v in got8.values()), (want8, got8)
+    assert len(set(got300.values())) == 1, got300
+
+
 def test_independent_contexts_interleaved():
     a = cl.LLContext(86243, 4096)
     b = cl.LLContext(132049, 7168)
