@@ -393,6 +393,7 @@ struct StaticTall {
   {LIST::L, tall_static<LIST>, LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, \
    tall_extra<LIST>(), tw_size<LIST>()}
 
+using L256 = RList<16, 16>;
 using L512 = RList<16, 2, 16>;
 using L768 = RList<16, 3, 16>;
 using L1024 = RList<16, 4, 16>;
@@ -407,12 +408,12 @@ using L3584 = RList<16, 14, 16>;
 using L4096 = RList<16, 16, 16>;
 
 static const StaticWide kWide[] = {
-    LLB_WIDE(L512, 4),  LLB_WIDE(L768, 4),  LLB_WIDE(L1024, 2), LLB_WIDE(L1280, 2),
+    LLB_WIDE(L256, 4),  LLB_WIDE(L512, 4),  LLB_WIDE(L768, 4),  LLB_WIDE(L1024, 2), LLB_WIDE(L1280, 2),
     LLB_WIDE(L1536, 2), LLB_WIDE(L1792, 2), LLB_WIDE(L2048, 2), LLB_WIDE(L2304, 2),
     LLB_WIDE(L2560, 1), LLB_WIDE(L3072, 1), LLB_WIDE(L3584, 1), LLB_WIDE(L4096, 1),
 };
 static const StaticTall kTall[] = {
-    LLB_TALL(L512),  LLB_TALL(L768),  LLB_TALL(L1024), LLB_TALL(L1280), LLB_TALL(L1536), LLB_TALL(L1792),
+    LLB_TALL(L256),  LLB_TALL(L512),  LLB_TALL(L768),  LLB_TALL(L1024), LLB_TALL(L1280), LLB_TALL(L1536), LLB_TALL(L1792),
     LLB_TALL(L2048), LLB_TALL(L2304), LLB_TALL(L2560), LLB_TALL(L3072), LLB_TALL(L3584), LLB_TALL(L4096),
 };
 

@@ -1,4 +1,5 @@
-// Compile-time specialised tall/wide passes for row lengths L = 16 * M.
+// Compile-time specialised tall/wide passes for row lengths L = 16 * M * 16
+// (radix list 16, M, 16) and L = 256 (16, 16).
 //
 // Same mathematics and data layout as the generic kernels in engine.cu, but
 // the radix list of the row transform is a template parameter, so every
@@ -270,7 +271,7 @@ template <class P>
 __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>())) tall_static(TallArgs a) {
   constexpr int H = P::L, TR = H / 16, T = 2 * TR, CS = col_slots<H>();
   constexpr bool kHalf = tall_half_exchange<P>();
-  static_assert(P::N == 3 && P::a[0] == 16 && P::a[2] == 16, "radix list 16, M, 16");
+  static_assert((P::N == 2 || P::N == 3) && P::a[0] == 16 && P::a[P::N - 1] == 16, "radix list 16, (M,) 16");
   extern __shared__ double2 sm[];
   double2 *stw = sm + padded(2 * H);
   double2 *wr = stw + tw_size<P>();  // w_N^(k*TR*r), both columns
@@ -286,13 +287,15 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
   const int col = threadIdx.x / TR, t = threadIdx.x - col * TR;
   const int k1 = col ? kB : kA;
   for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
-  if (threadIdx.x < 32) {
-    const int kk = threadIdx.x < 16 ? kA : kB, r = threadIdx.x & 15;
-    wr[threadIdx.x] = omegaN(a.thi, a.tlo, a.ts, a.tmask, kk * TR * r);
-  } else if (threadIdx.x < 40) {
-    pj[threadIdx.x - 32] = __ldg(&a.twH[(threadIdx.x - 32) * T]);
-  } else if (kHalf && threadIdx.x < 56) {
-    fr[threadIdx.x - 40] = __ldg(&a.twH[(threadIdx.x - 40) * TR]);
+  for (int i = threadIdx.x; i < (kHalf ? 56 : 40); i += T) {  // one pass when T >= 56
+    if (i < 32) {
+      const int kk = i < 16 ? kA : kB, r = i & 15;
+      wr[i] = omegaN(a.thi, a.tlo, a.ts, a.tmask, kk * TR * r);
+    } else if (i < 40) {
+      pj[i - 32] = __ldg(&a.twH[(i - 32) * T]);
+    } else {
+      fr[i - 40] = __ldg(&a.twH[(i - 40) * TR]);
+    }
   }
   // with the half exchange the per-thread twiddle bases are parked in the
   // thread's own shared-memory slot while the transforms hold the registers

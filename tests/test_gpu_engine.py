@@ -152,6 +152,9 @@ def test_c3_18432k_matches_exact_and_reference_binary():
     # N = 1280*768: columns of 768 and 1280 (threads of both columns in one
     # warp), rows of 1280 and 768
     (34603069, 1966080, [768, 1280, None]),
+    # N = 256*512: the two-stage (16, 16) rows and columns of 256
+    (4587533, 262144, [256, 512, None]),
+    (2293771, 131072, [256, None]),
 ])
 def test_kernel_variants_agree(q, n, widths):
     """Every launch shape of one length (specialised kernels for several row
