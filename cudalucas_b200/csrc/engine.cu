@@ -410,7 +410,7 @@ using L4096 = RList<16, 16, 16>;
 static const StaticWide kWide[] = {
     LLB_WIDE(L256, 4),  LLB_WIDE(L512, 4),  LLB_WIDE(L768, 4),  LLB_WIDE(L1024, 2), LLB_WIDE(L1280, 2),
     LLB_WIDE(L1536, 2), LLB_WIDE(L1792, 2), LLB_WIDE(L2048, 2), LLB_WIDE(L2304, 2),
-    LLB_WIDE(L2560, 1), LLB_WIDE(L3072, 1), LLB_WIDE(L3584, 1), LLB_WIDE(L4096, 1),
+    LLB_WIDE(L2560, 2), LLB_WIDE(L3072, 2), LLB_WIDE(L3584, 1), LLB_WIDE(L4096, 1),
 };
 static const StaticTall kTall[] = {
     LLB_TALL(L256),  LLB_TALL(L512),  LLB_TALL(L768),  LLB_TALL(L1024), LLB_TALL(L1280), LLB_TALL(L1536), LLB_TALL(L1792),
