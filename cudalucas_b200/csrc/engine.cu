@@ -550,6 +550,27 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
       out.st = bt;
       return true;
     }
+    // a specialised wide pass with the generic tall pass, when the columns
+    // have no specialised length (the wide pass is the costlier one)
+    for (const auto &w : kWide) {
+      if (N % w.L) continue;
+      if (t && t->width > 0 && t->width != w.L) continue;
+      const long long H = N / w.L;
+      Shape s;
+      if (H % w.G || !shape_ok(N, w.L, w.G, s) || s.T2 > TMAX || s.H > EPT * s.T2) continue;
+      const double d = fabs(log((double)w.L / sqrt((double)N)));
+      if (d < best) {
+        best = d;
+        bw = &w;
+        out = s;
+      }
+    }
+    if (bw) {
+      out.T1 = bw->G * (bw->L / 16);
+      out.sw = bw;
+      out.st = nullptr;
+      return true;
+    }
   }
   std::vector<int> ws;
   if (t && t->width > 0) ws.push_back(t->width);

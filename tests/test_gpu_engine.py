@@ -47,8 +47,11 @@ def test_parity_with_oracle(q, n):
 
 @pytest.mark.parametrize("q,n", [(86243, 4096), (216091, 12288), (1257787, 65536)])
 def test_digits_match_engine_model_bit_for_bit(q, n):
+    # the model follows the generic kernels' carry (c2 added after balancing);
+    # the specialised wide pass adds c1 + c2 before, which gives other digits
+    # of the same value (checked by the parity tests)
     off = q // 7
-    d, _, _, shape = engine_run(q, n, off, 25)
+    d, _, _, shape = engine_run(q, n, off, 25, rows_per_cta=2)
     m = ibdwt_model.Model(q, n, shape["W"])
     m.start(off)
     for _ in range(25):
