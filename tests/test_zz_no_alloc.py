@@ -28,7 +28,8 @@ def static_step(q, n, offset, iters, d_in, d_out):
 
 
 @pytest.mark.parametrize("q,n,k1,k2", [(86243, 4096, 300, 700), (216091, 12288, 500, 250),
-                                       (1257787, 65536, 120, 80)])
+                                       (1257787, 65536, 120, 80),
+                                       (18454939, 1 << 20, 30, 20)])  # the stated maximum size
 def test_static_entry_point_matches_context_entry_point(q, n, k1, k2):
     import torch
     off0 = (q * 3) // 7
@@ -37,6 +38,13 @@ def test_static_entry_point_matches_context_entry_point(q, n, k1, k2):
         d0, o0 = c.read_digits()
         e1 = c.step(k1, report=True)
         d1, o1 = c.read_digits()
+        # The static entry point starts every call from loaded digits.  A
+        # context that goes on after a report step starts from the report
+        # pass's own floating-point state, which another kernel instantiation
+        # computes and which can differ in the last bits (same digits, a
+        # different roundoff maximum on the next iteration); so the reference
+        # reloads its digits too.
+        c.load_digits(d1, o1)
         e2 = c.step(k2, report=True)
         d2, o2 = c.read_digits()
     dev_in = torch.from_numpy(d0.copy()).cuda()
