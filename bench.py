@@ -347,7 +347,7 @@ def run_batch(args, world, rank, local):
     members = workloads.batch_exponents(args.batch_count, seed=7 + rank)
     qs, ns = zip(*members)
     S, K, W = args.iters_per_step, args.steps, args.warmup
-    b = cl.LLBatch(qs, ns, device=local, graph_iters=10)
+    b = cl.LLBatch(qs, ns, device=local, graph_iters=args.batch_graph_iters)
     b.start([(q * 7) // 11 for q in qs])
     for _ in range(W):
         b.step(S)
@@ -393,7 +393,7 @@ def run_batch(args, world, rank, local):
         "dtype": "f64", "data": "synthetic: seeded exponents, LL tests from s0=4",
         "config": {"workload": "batch: %d primes log-uniform in [1e6, 2e7] (seed 7), lengths %dK..%dK"
                                % (len(members), min(ns) // 1024, max(ns) // 1024),
-                   "iters_per_step": S, "graph_iters": 10,
+                   "iters_per_step": S, "graph_iters": args.batch_graph_iters,
                    "serial_iter_s": round(serial_ips, 1), "speedup_vs_serial": round(batch_ips / serial_ips, 3),
                    "serial_sample": "%d iterations of each exponent alone" % Ss,
                    "max_roundoff_error": round(float(max(errs)), 5),
@@ -452,6 +452,8 @@ def main():
     ap.add_argument("--serve-count", type=int, default=32)
     ap.add_argument("--serve-chunk", type=int, default=1000)
     ap.add_argument("--batch-count", type=int, default=256)
+    ap.add_argument("--batch-graph-iters", type=int, default=10,
+                    help="iterations of every member per CUDA graph in the batch workload")
     ap.add_argument("--serial-iters", type=int, default=200)
     ap.add_argument("--iters-per-step", type=int, default=10000)
     ap.add_argument("--cpu-iters", type=int, default=20, help="oracle iterations for cpu_baseline (0: skip)")
