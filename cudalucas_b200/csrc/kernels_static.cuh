@@ -253,7 +253,7 @@ __host__ __device__ constexpr int tall_extra() {
   return tw_size<P>() + 32 + 8 + (tall_half_exchange<P>() ? 16 + 4 * (P::L / 16) : 0);
 }
 
-// Tall pass for columns of length H = P::L (radix list 16, M, 16); two
+// Tall pass for columns of length H = P::L (radix list 16, M, 16 or 16, 16); two
 // columns per CTA.
 // The column twiddle w_N^(k1*m2) of element m2 = t + r*TR is formed as
 // w_N^(k1*t) (one table product per thread) times w_N^(k1*TR*r) (shared by
