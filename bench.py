@@ -138,19 +138,44 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_baseline(q, n, iters):
-    """The oracle (plain C IBDWT restatement, one host core) on a bounded
-    sample of the same workload."""
-    from oracle.binding import Oracle
-    o = Oracle(q, n)
-    o.start(0)
-    o.step(1)
-    t = time.perf_counter()
-    o.step(iters)
-    dt = time.perf_counter() - t
-    return {"value": dt * 1000.0 / iters, "unit": "ms/iter", "cores": 1, "kind": "port",
-            "sample": "%d iterations of p=%d at n=%d (oracle/ibdwt_oracle.c, mixed-radix C FFT, 1 thread)"
-                      % (iters, q, n)}
+def cpu_baseline(q, n, iters1, iters_all):
+    """The oracle (plain C IBDWT restatement) timed on this machine's host
+    cores on a bounded sample of the same workload: one thread, then all the
+    cores this process may use (POSIX threads over the independent
+    butterflies, pairs and carry blocks)."""
+    from oracle.binding import Oracle, set_threads
+    cores = len(os.sched_getaffinity(0))
+
+    def timed(threads, iters):
+        set_threads(threads)
+        o = Oracle(q, n)
+        o.start(0)
+        o.step(1)
+        t = time.perf_counter()
+        o.step(iters)
+        return (time.perf_counter() - t) * 1000.0 / iters
+
+    ms1 = timed(1, iters1)
+    msn = timed(cores, iters_all)
+    set_threads(1)
+    return {"value": round(msn, 3), "unit": "ms/iter", "cores": cores, "kind": "port",
+            "sample": "%d iterations of p=%d at n=%d from s0=4 (oracle/ibdwt_oracle.c, mixed-radix C FFT, "
+                      "%d POSIX threads)" % (iters_all, q, n, cores),
+            "single_core": {"value": round(ms1, 3), "unit": "ms/iter", "cores": 1,
+                            "sample": "%d iterations, 1 thread" % iters1}}
+
+
+def reference_res64(q, n):
+    """{iteration: Res64} printed by the reference binary itself for this
+    exponent and length (committed fixtures tests/golden/ref_*_res64.json)."""
+    out = {}
+    gdir = os.path.join(ROOT, "tests", "golden")
+    for name in sorted(os.listdir(gdir)):
+        if name.startswith("ref_") and name.endswith("_res64.json"):
+            d = json.load(open(os.path.join(gdir, name)))
+            if d.get("exponent") == q and d.get("fft_words") == n:
+                out.update({int(k): int(r, 16) for _, k, r in d["entries"]})
+    return out
 
 
 def run_ours(args, world, rank, local):
@@ -165,10 +190,21 @@ def run_ours(args, world, rank, local):
     ctx.start((rank * 7919) % q)
     ext = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+    want = reference_res64(q, n)
+    got = {}
+    done = 0
 
+    def check_step():
+        # the step's last iteration wrote the digits (LL_REPORT): Res64 of
+        # the state after `done` iterations, read after the step's events
+        d, off = ctx.read_digits()
+        got[done] = cl.digits_res64(d, q, n, off)
+
+    # every step, warm-up and timed, is S iterations whose last one reports
     for _ in range(W):
-        ctx.step(S)
-    ctx.sync()
+        ctx.step(S, report=True, wait=False)
+        done += S
+        check_step()
 
     # -- device-timed region: K steps of S iterations, L2 flushed between steps
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
@@ -179,14 +215,18 @@ def run_ours(args, world, rank, local):
             with torch.cuda.stream(ext):
                 flush.zero_()
                 evs[i][0].record(ext)
-            ctx.step(S)
+            ctx.step(S, report=True, wait=False)
             evs[i][1].record(ext)
+            done += S
+            check_step()
         ctx.sync()
         torch.cuda.synchronize()
     barrier(world)
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = allreduce_max(sum(step_ms), world)
-    maxerr = ctx.step(1, report=True)
+    maxerr = ctx.step(0, errchk=True)  # max over every iteration so far
+    d_last, off_last = ctx.read_digits()
+    it_last = done
 
     # -- per-pass timing on real iterations (roofline of the dominant kernel)
     R = 200
@@ -203,10 +243,9 @@ def run_ours(args, world, rank, local):
     t_wide = sum(e[1].elapsed_time(e[2]) for e in ev) / R
 
     # -- end to end through the public API with host buffers (pinned):
-    # load digits (H2D), S iterations, read digits (D2H), Res64 on the host
-    ctx.step(1, report=True)
-    d0, off0 = ctx.read_digits()
-    pinned_in = torch.from_numpy(d0).pin_memory()
+    # load digits (H2D), S iterations, read digits (D2H), Res64 on the host;
+    # every repetition continues from the state after the timed steps
+    pinned_in = torch.from_numpy(d_last).pin_memory()
     pinned_out = torch.empty(n, dtype=torch.int32).pin_memory()
     import ctypes
     from cudalucas_b200 import native
@@ -216,20 +255,34 @@ def run_ours(args, world, rank, local):
     offv = ctypes.c_uint32()
     errv = ctypes.c_float()
     E = max(1, min(K, 3))
+    e2e_res = []
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(E):
-        assert L.ll_load_digits(ctx._h, pin_in, off0) == 0
+        assert L.ll_load_digits(ctx._h, pin_in, off_last) == 0
         assert L.ll_step(ctx._h, S, 1, ctypes.byref(errv)) == 0
         assert L.ll_read_digits(ctx._h, pin_out, ctypes.byref(offv)) == 0
-        res = L.ll_digits_res64(pin_out, q, n, offv.value)
+        e2e_res.append(L.ll_digits_res64(pin_out, q, n, offv.value))
     e2e_ms = (time.perf_counter() - t0) * 1000.0
     e2e_ms = allreduce_max(e2e_ms, world)
+    got_e2e = e2e_res[0]
     shape = ctx.shape
     ctx.close()
 
+    # -- parity: Res64 after every step against the reference binary's own
+    # report lines for this exponent and length (rank 0 starts at offset 0,
+    # the others at other offsets; Res64 does not depend on the offset)
+    checked = {k: v for k, v in got.items() if k in want}
+    mismatched = sorted(k for k, v in checked.items() if want[k] != v)
+    e2e_consistent = len(set(e2e_res)) == 1
+    e2e_checked = (it_last + S) in want
+    if e2e_checked and want[it_last + S] != got_e2e:
+        mismatched.append(it_last + S)
+    ok = not mismatched and e2e_consistent
+    ok_all = allreduce_max(0.0 if ok else 1.0, world) == 0.0
+
     if rank != 0:
-        return None
+        return None if ok_all else {"fail": True}
     hbm, peak_kind = peaks()
     dom, t_dom = ("wide", t_wide) if t_wide >= t_tall else ("tall", t_tall)
     alg_bytes = 16.0 * n  # one read + one write of n FP64 words per pass
@@ -255,9 +308,15 @@ def run_ours(args, world, rank, local):
                    "l2": "flushed (256 MB write) before each timed step; the 26 MB state stays "
                          "L2-resident inside a step, as it does for the reference",
                    "parallelism": "replicas (one independent exponent per GPU)"},
+        "res64_ok": ok_all,
+        "res64": {str(k): "%016x" % v for k, v in sorted(got.items())},
+        "res64_checked": {"against": "Res64 printed by the reference binary (tests/golden/ref_*_res64.json)",
+                          "iterations": sorted(checked) + ([it_last + S] if e2e_checked else []),
+                          "mismatched": mismatched, "e2e_repetitions_agree": e2e_consistent},
         "e2e": {"value": round(e2e_ms / (E * S * world), 6) * world, "unit": "ms/iter",
                 "h2d_bytes_per_step": 4 * n + 32, "d2h_bytes_per_step": 4 * n + 32,
-                "steps": E, "path": "ll_load_digits -> ll_step(LL_REPORT) -> ll_read_digits -> ll_digits_res64"},
+                "steps": E, "res64": "%016x" % got_e2e, "iteration": it_last + S,
+                "path": "ll_load_digits -> ll_step(LL_REPORT) -> ll_read_digits -> ll_digits_res64"},
         "roofline": {"bound": "hbm", "kernel": dom + "_kernel", "achieved": round(achieved, 1),
                      "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
@@ -266,7 +325,7 @@ def run_ours(args, world, rank, local):
         "gpu_launches": 2 * K * S,
     }
     if args.cpu_iters > 0:
-        out["cpu_baseline"] = cpu_baseline(q, n, args.cpu_iters)
+        out["cpu_baseline"] = cpu_baseline(q, n, args.cpu_iters, args.cpu_iters_all)
     return out
 
 
@@ -329,9 +388,11 @@ def run_reference(args, world, rank, local):
                    "timing": "CUDALucas's own wall-clock ms/iter per report interval (includes its "
                              "blocking error read-back every 100 iterations, CUDALucas.cu:2936)"},
         "e2e": {"value": round(ms, 6), "unit": "ms/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "cpu_baseline": {"value": round(ms, 6), "unit": "ms/iter", "cores": 1, "kind": "reference",
-                         "sample": "%d report intervals of %d iterations of the reference binary "
-                                   "(GPU %d, driven by one host thread)" % (K, S, local)},
+        "reference_run": {"value": round(ms, 6), "unit": "ms/iter", "kind": "reference", "device": "gpu",
+                          "host_threads": 1,
+                          "sample": "%d report intervals of %d iterations of the reference binary, a GPU "
+                                    "program (cuFFT path on GPU %d); it has no host-core implementation"
+                                    % (K, S, local)},
     })
     return base
 
@@ -456,7 +517,10 @@ def main():
                     help="iterations of every member per CUDA graph in the batch workload")
     ap.add_argument("--serial-iters", type=int, default=200)
     ap.add_argument("--iters-per-step", type=int, default=10000)
-    ap.add_argument("--cpu-iters", type=int, default=20, help="oracle iterations for cpu_baseline (0: skip)")
+    ap.add_argument("--cpu-iters", type=int, default=20,
+                    help="oracle iterations on one host thread for cpu_baseline (0: skip)")
+    ap.add_argument("--cpu-iters-all", type=int, default=100,
+                    help="oracle iterations on all host cores for cpu_baseline")
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.workload == "serve":
@@ -469,11 +533,14 @@ def main():
         out = run_reference(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
-    if out is not None:
+    failed = out is not None and (out.get("fail") or out.get("res64_ok") is False)
+    if out is not None and not out.get("fail"):
         print(json.dumps(out), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+    if failed:
+        sys.exit("Res64 differs from the reference binary's")
 
 
 if __name__ == "__main__":

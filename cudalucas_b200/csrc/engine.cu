@@ -279,6 +279,8 @@ __global__ void __launch_bounds__(256) wide_kernel(WideArgs a) {
         const double r0 = rint(t0), r1 = rint(t1);
         emax = fmaxf(emax, fabsf((float)(t0 - r0)));
         emax = fmaxf(emax, fabsf((float)(t1 - r1)));
+        // no fraction bits left for the roundoff reading at 2^51 and above (or NaN)
+        if (!(fabs(t0) < 0x1p51 && fabs(t1) < 0x1p51)) fault |= 2u;
         long long v0 = (long long)r0, v1 = (long long)r1;
         const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
         if (j0 == dw) v0 -= sub;
@@ -1014,7 +1016,7 @@ ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
     if (rc != LL_OK) return rc;
   }
   if (iters) ctx->digits_current = report;
-  if (flags & (LL_REPORT | LL_ERRCHK)) {
+  if ((flags & (LL_REPORT | LL_ERRCHK)) && !(flags & LL_ASYNC)) {
     DevState hs{};
     CK(cudaMemcpyAsync(&hs, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1032,7 +1034,7 @@ ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
       return LL_ERR_TIMEOUT;
     }
     if (hs.fault & 2u) {
-      ctx->err = "wide pass: carry out of range (roundoff far above 0.5)";
+      ctx->err = "wide pass: a word beyond the exact FP64 range (roundoff far above 0.5, or digits out of range)";
       if (max_err) *max_err = 1.0f;
     }
   }
@@ -1108,6 +1110,14 @@ ll_status ll_debug_launch(ll_ctx *ctx, int32_t which) {
   return LL_OK;
 }
 
+int32_t ll_device_name(int device, char *name, size_t len) {
+  if (!name || !len) return -1;
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return -1;
+  snprintf(name, len, "%s", p.name);
+  return 0;
+}
+
 int32_t ll_length_supported(uint32_t n) {
   if (n < 64 || n % 4) return 0;
   Shape s;
@@ -1134,11 +1144,18 @@ static __device__ __align__(256) unsigned char g_ll_scratch[kScratchBytes];
 
 namespace {
 
-// Host-side table staging, also file-scope so that no call allocates.
+// Host-side table staging, also file-scope so that no call allocates.  It is
+// guarded by g_table_mu only while the tables are built and copied: a copy
+// from pageable host memory has consumed its source when cudaMemcpyAsync
+// returns.  Each device's scratch is guarded by that device's own mutex, held
+// until the call's work on the GPU has finished, so calls on different GPUs
+// do not wait for each other's kernels.
+constexpr int kMaxDevices = 64;
 constexpr size_t kHostTableBytes = 2u << 20;
 alignas(256) unsigned char g_host_tables[kHostTableBytes];
-std::mutex g_static_mu;
-void *g_scratch_ptr[64] = {nullptr};  // device address of g_ll_scratch, per device
+std::mutex g_table_mu;
+std::mutex g_device_mu[kMaxDevices];
+void *g_scratch_ptr[kMaxDevices] = {nullptr};  // device address of g_ll_scratch, per device
 
 size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
@@ -1158,19 +1175,28 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
                                     void *stream) {
   if (!digits_in || !digits_out || n < 64 || n % 4 || q <= n || (q & 1) == 0 || offset >= q) return LL_ERR_ARG;
   if (n > LL_STATIC_MAX_WORDS) return LL_ERR_ARG;  // beyond the static scratch's stated maximum
-  if (device < 0 || device >= 64) return LL_ERR_ARG;
+  if (device < 0 || device >= kMaxDevices) return LL_ERR_ARG;
   const int N = (int)(n / 2);
   Shape s;
   if (!choose_shape(N, nullptr, s)) return LL_ERR_SHAPE;
-  std::lock_guard<std::mutex> lock(g_static_mu);
+  std::lock_guard<std::mutex> lock(g_device_mu[device]);
   int prev = 0;
   cudaGetDevice(&prev);
   if (cudaSetDevice(device) != cudaSuccess) return LL_ERR_CUDA;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Declared after the lock, so destroyed before it: on every return, work
+  // this call has enqueued finishes before another call may reuse the
+  // scratch, and the caller's current device is put back.
   struct Restore {
     int d;
-    ~Restore() { cudaSetDevice(d); }
-  } restore{prev};
-  cudaStream_t st = (cudaStream_t)stream;
+    cudaStream_t s;
+    bool enqueued = false;
+    ~Restore() {
+      if (enqueued) cudaStreamSynchronize(s);
+      cudaSetDevice(d);
+    }
+  } restore{prev, st};
+  std::unique_lock<std::mutex> table_lock(g_table_mu);
   // set-up, once per device: the device address of the static array
   if (!g_scratch_ptr[device]) {
     void *p = nullptr;
@@ -1304,10 +1330,12 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
   // ---- state that must start at zero: flags, ticket, error, fault
   DevState hs{};
   hs.offset = offset;
+  restore.enqueued = true;
   if ((e = cudaMemsetAsync(flags, 0, sizeof(uint32_t) * kWarpFlags * (size_t)ngroups, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(dst, &hs, sizeof(DevState), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
       (e = cudaMemcpyAsync(dtab, g_host_tables, table_bytes, cudaMemcpyHostToDevice, st)) != cudaSuccess)
     return LL_ERR_CUDA;
+  table_lock.unlock();  // the pageable-source copies above have consumed the host tables
 
   // ---- digits in -> weighted transform -> iters iterations -> digits out
   const dim3 gw(H / s.G), gt(W / 2);
@@ -1331,8 +1359,13 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
   if ((e = cudaMemcpyAsync(&hs, dst, sizeof(DevState), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
       (e = cudaStreamSynchronize(st)) != cudaSuccess)
     return LL_ERR_CUDA;
+  restore.enqueued = false;
   if (max_err) memcpy(max_err, &hs.err_bits, sizeof(float));
   if (hs.fault & 1u) return LL_ERR_TIMEOUT;
+  // a word outside the exact FP64 range: the digits are not valid, and the
+  // roundoff reading may not show it; report it as ll_step does, as the
+  // largest possible error, so that the caller's roundoff policy fires
+  if ((hs.fault & 2u) && max_err) *max_err = 1.0f;
   return LL_OK;
 }
 

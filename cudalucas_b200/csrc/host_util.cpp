@@ -6,6 +6,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <mutex>
 #include <vector>
 
 #include "../../include/llb200.h"
@@ -208,25 +209,103 @@ static const uint32_t k_default_mult[] = {
     42336, 43200, 43904, 47628, 49000, 50000, 50176, 51200, 52488, 54432, 55296, 56000, 57344, 60750, 62500,
     64000, 64800, 65536};
 
-int32_t ll_fft_table(uint32_t *lengths, int32_t max_count) {
-  const int32_t cnt = (int32_t)(sizeof(k_default_mult) / sizeof(k_default_mult[0]));
-  if (lengths)
-    for (int32_t i = 0; i < cnt && i < max_count; ++i) lengths[i] = k_default_mult[i] * 1024u;
-  return cnt;
+// The active length table: the built-in table, or the built-in table merged
+// with a measured list (ll_fft_table_merge), as init_ffts builds g_ffts from
+// `<gpu> fft.txt` (CUDALucas.cu:975-1021).  Guarded for callers on several
+// host threads.
+static std::mutex g_table_mu;
+static std::vector<uint32_t> g_table;  // empty: the built-in table
+
+static std::vector<uint32_t> active_table() {
+  std::lock_guard<std::mutex> lock(g_table_mu);
+  if (!g_table.empty()) return g_table;
+  std::vector<uint32_t> t;
+  for (uint32_t m : k_default_mult) t.push_back(m * 1024u);
+  return t;
 }
 
-// choose_fft_length (CUDALucas.cu:1027-1068) without a <gpu> fft.txt file:
-// the smallest table length >= max(lb, want) that the engine supports,
-// clamped to the upper bound.  A `want` that is not in the table is used as
-// is when it lies within the bounds (init_ffts inserts it, CUDALucas.cu:995).
+int32_t ll_fft_table(uint32_t *lengths, int32_t max_count) {
+  const std::vector<uint32_t> t = active_table();
+  if (lengths)
+    for (int32_t i = 0; i < (int32_t)t.size() && i < max_count; ++i) lengths[i] = t[(size_t)i];
+  return (int32_t)t.size();
+}
+
+// init_ffts (CUDALucas.cu:947-1022): the built-in lengths below the smallest
+// measured length, then the measured lengths (ascending, as the benchmark
+// writes them), then the built-in lengths above the largest measured one.
+// Inside the measured range only measured lengths remain, so a length the
+// benchmark found slower than a longer one is never chosen.  count == 0
+// restores the built-in table.
+int32_t ll_fft_table_merge(const uint32_t *measured, int32_t count) {
+  if (count < 0 || (count > 0 && !measured)) return -1;
+  std::vector<uint32_t> m;
+  for (int32_t i = 0; i < count; ++i)
+    if (measured[i] && (m.empty() || measured[i] > m.back())) m.push_back(measured[i]);
+  std::vector<uint32_t> t;
+  if (!m.empty()) {
+    for (uint32_t d : k_default_mult)
+      if (d * 1024u < m.front()) t.push_back(d * 1024u);
+    t.insert(t.end(), m.begin(), m.end());
+    for (uint32_t d : k_default_mult)
+      if (d * 1024u > m.back()) t.push_back(d * 1024u);
+  }
+  std::lock_guard<std::mutex> lock(g_table_mu);
+  g_table = t;
+  return (int32_t)(t.empty() ? sizeof(k_default_mult) / sizeof(k_default_mult[0]) : t.size());
+}
+
+// The pruning of -cufftbench (CUDALucas.cu:2500-2513): scanning from the
+// longest length down, a length is kept when it is faster than every longer
+// length; lengths that are powers of two (in K) are always kept.
+int32_t ll_fft_prune(const uint32_t *lengths, const float *ms_per_iter, int32_t count, int32_t *keep) {
+  if (count < 0 || (count > 0 && (!lengths || !ms_per_iter || !keep))) return -1;
+  float best = 0.f;
+  bool any = false;
+  int32_t kept = 0;
+  for (int32_t i = count - 1; i >= 0; --i) {
+    const uint32_t k = lengths[i] / 1024u;
+    const bool pow2 = k && (k & (k - 1)) == 0 && lengths[i] % 1024u == 0;
+    keep[i] = 0;
+    if (ms_per_iter[i] > 0.f && (!any || ms_per_iter[i] < best)) {
+      best = ms_per_iter[i];
+      any = true;
+      keep[i] = 1;
+    } else if (pow2 && ms_per_iter[i] > 0.f) {
+      keep[i] = 1;
+    }
+    kept += keep[i];
+  }
+  return kept;
+}
+
+// Largest exponent whose lower length bound (ll_fft_bounds) is at most n:
+// the `max exp` column of `<gpu> fft.txt`.
+uint32_t ll_fft_max_exponent(uint32_t n) {
+  const double ff1 = 0.999 * 1024.0 * 0.0000357822505975293;
+  const double e1 = 1.022179977969700;
+  double qmax = exp(log((double)n / ff1) / e1);
+  uint32_t q = qmax >= 4294967295.0 ? 0xfffffffdu : (uint32_t)qmax;
+  uint32_t lb = 0;
+  while (q > 3) {
+    ll_fft_bounds(q, &lb, nullptr);
+    if (lb <= n) break;
+    --q;
+  }
+  return q;
+}
+
+// choose_fft_length (CUDALucas.cu:1027-1068): the smallest table length >=
+// max(lb, want) that the engine supports, clamped to the upper bound.  A
+// `want` that is not in the table is used as is when it lies within the
+// bounds (init_ffts inserts it, CUDALucas.cu:995).
 uint32_t ll_choose_fft_length(uint32_t q, uint32_t want) {
   uint32_t lb = 0, ub = 0;
   ll_fft_bounds(q, &lb, &ub);
   if (want && want >= lb && want <= ub && ll_length_supported(want)) return want;
-  const int32_t cnt = (int32_t)(sizeof(k_default_mult) / sizeof(k_default_mult[0]));
+  const std::vector<uint32_t> t = active_table();
   const uint32_t lo = want > lb ? want : lb;
-  for (int32_t i = 0; i < cnt; ++i) {
-    const uint32_t n = k_default_mult[i] * 1024u;
+  for (uint32_t n : t) {
     if (n < lo) continue;
     if (n > ub) break;
     if (ll_length_supported(n) && q > n) return n;

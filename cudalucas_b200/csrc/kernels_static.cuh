@@ -465,6 +465,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   const double ip2lo = 1.0 / p2lo, ip2hi = 0.5 * ip2lo;
   double2 x[16];
   double emax = 0.0;
+  bool out_of_range = false;
   double Wi0 = 0.0, Wi1 = 0.0;
   if (MODE != WIDE_INIT) {
     const double cwit = __ldg(&a.colWi[t]);
@@ -524,6 +525,9 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
       const double t1 = u[r].y * (Wi1 * (n1 ? a.colSi2[r] : a.colSi[r]));
       double r0 = rint(t0), r1 = rint(t1);
       emax = fmax(emax, fmax(fabs(t0 - r0), fabs(t1 - r1)));
+      // at 2^51 and above (or NaN) a double has no fraction bits left for the
+      // roundoff reading, and the exact carry split below no longer holds
+      if (!(fabs(t0) < 0x1p51 && fabs(t1) < 0x1p51)) out_of_range = true;
       if (r == r_sub) {
         if (w_sub) r1 -= sub;
         else r0 -= sub;
@@ -630,6 +634,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
 #pragma unroll
     for (int o = 16; o; o >>= 1) em = fmaxf(em, __shfl_xor_sync(0xffffffffu, em, o));
     if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = em;
+    if (out_of_range) atomicOr(&s_fault, 2u);
     __syncthreads();
     if (threadIdx.x == 0) {
       float m = 0.f;

@@ -68,11 +68,16 @@ class LLContext:
         assert d.size == self.n
         self._check(native.lib().ll_load_digits(self._h, _i32p(d), int(offset)), "ll_load_digits")
 
-    def step(self, iters, report=False, errchk=False):
+    def step(self, iters, report=False, errchk=False, wait=True):
+        """iters LL iterations; returns the max roundoff error when a flag
+        asks for it and wait is true.  wait=False only enqueues (LL_ASYNC):
+        with report=True the digits are readable once the work finishes."""
         e = ctypes.c_float(0)
         flags = (LL_REPORT if report else 0) | (LL_ERRCHK if errchk else 0)
+        if not wait:
+            flags |= native.LL_ASYNC
         self._check(native.lib().ll_step(self._h, int(iters), flags, ctypes.byref(e)), "ll_step")
-        return float(e.value) if flags else None
+        return float(e.value) if flags and wait else None
 
     def read_digits(self):
         d = np.zeros(self.n, dtype=np.int32)
@@ -240,3 +245,32 @@ def fft_table():
 
 def length_supported(n):
     return bool(native.lib().ll_length_supported(n))
+
+
+def fft_table_merge(measured):
+    """Installs the built-in table merged with measured lengths (ascending,
+    in words), as init_ffts does with `<gpu> fft.txt`; [] restores the
+    built-in table.  Returns the new table size."""
+    m = np.ascontiguousarray(sorted(int(x) for x in measured), dtype=np.uint32)
+    return int(native.lib().ll_fft_table_merge(_u32p(m) if m.size else None, int(m.size)))
+
+
+def fft_prune(lengths, ms_per_iter):
+    """The -cufftbench pruning rule: which lengths (ascending) to keep."""
+    n = np.ascontiguousarray(lengths, dtype=np.uint32)
+    t = np.ascontiguousarray(ms_per_iter, dtype=np.float32)
+    keep = np.zeros(n.size, dtype=np.int32)
+    native.lib().ll_fft_prune(_u32p(n), t.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), int(n.size),
+                              _i32p(keep))
+    return [bool(k) for k in keep]
+
+
+def fft_max_exponent(n):
+    return int(native.lib().ll_fft_max_exponent(int(n)))
+
+
+def device_name(device=0):
+    buf = ctypes.create_string_buffer(256)
+    if native.lib().ll_device_name(int(device), buf, 256):
+        raise LLError(native.LL_ERR_CUDA, "ll_device_name(%d)" % device)
+    return buf.value.decode()

@@ -22,6 +22,7 @@
 #include <time.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -44,11 +45,20 @@ struct Config {
   int polite = 0, polite_value = 50;
   int error_reset = 85;
   int error_limit = 40;     // ErrorLimit (percent)
-  int roundoff_test = 0;
+  int roundoff_test = 0;    // RoundoffTest
   int selftest = -1;        // -r
   uint32_t fft_len = 0;     // -f / FFTLength
   bool quiet_ini = false;
+  // Fault-injection hook for the recovery tests: LLUCAS_INJECT_FAILURES=J:C
+  // makes the C ll_step calls made once the test reaches iteration J fail
+  // on the host (ll_debug_inject_failure), once per process.
+  uint32_t inject_at = 0;
+  int inject_count = 0;
 };
+
+static bool g_injected = false;
+
+static bool shape_for(const Config &cfg, uint32_t n, ll_tuning &tu);
 
 static volatile sig_atomic_t g_quit = 0;
 static void on_signal(int) { g_quit = 1; }
@@ -345,6 +355,56 @@ static uint32_t next_length(uint32_t q, uint32_t n) {
 // check(q): one LL test with checkpoints, reports and the roundoff policy
 // (CUDALucas.cu:2862-3186).  Returns 0 on completion, 1 when interrupted,
 // 2 on an unrecoverable error.
+// round_off_test (CUDALucas.cu:2589-2648): 1000 iterations with the error
+// read back after every one.  Returns 1 when the average error exceeds 0.25
+// or one iteration exceeds 0.35 (the caller moves to a longer FFT), 0 when
+// the test may continue from the state reached (j and offset advanced, the
+// last iteration reported), -1 on an engine error.
+static int round_off_test(ll_ctx *c, uint32_t q, uint32_t n, uint32_t &j, uint32_t &offset) {
+  printf("Running careful round off test for 1000 iterations.\n");
+  printf("If average error > 0.25, or maximum error > 0.35,\n");
+  printf("the test will restart with a longer FFT.\n");
+  fflush(stdout);
+  const uint32_t last = q - 2;
+  float total = 0.f, max_err = 0.f, max_err1 = 0.f;
+  uint32_t k = 0;
+  const uint32_t count = last >= j ? std::min<uint32_t>(1000, last - j + 1) : 0;
+  for (; k < count; ++k) {
+    float e = 0.f;
+    const ll_status s = ll_step(c, 1, k + 1 == count ? LL_REPORT : LL_ERRCHK, &e);
+    if (s != LL_OK) { fail(c, s, "ll_step"); return -1; }
+    if (e > max_err) max_err = e;
+    if (e > max_err1) max_err1 = e;
+    total += e;
+    if (e > 0.35f) {
+      printf("Iteration = %u < 1000 && err = %5.5f > 0.35, increasing n from %uK\n", k, e, n / 1024);
+      return 1;
+    }
+    if (k && k % 100 == 0) {
+      printf("Iteration  %u, average error = %5.5f, max error = %5.5f\n", k, total / k, max_err);
+      max_err = 0.f;
+    }
+  }
+  const float avg = total / 1000.0f;
+  if (avg > 0.25f) {
+    printf("Iteration 1000, average error = %5.5f > 0.25 (max error = %5.5f), increasing FFT length and "
+           "restarting\n", avg, max_err);
+    return 1;
+  }
+  printf("Iteration 1000, average error = %5.5f <= 0.25 (max error = %5.5f), continuing test.\n", avg, max_err1);
+  offset = ll_offset(c);
+  j += k;
+  return 0;
+}
+
+// Applies the LLUCAS_INJECT_FAILURES hook once the test has reached it.
+static void maybe_inject(const Config &cfg, ll_ctx *c, uint32_t j) {
+  if (!g_injected && cfg.inject_count > 0 && j >= cfg.inject_at) {
+    ll_debug_inject_failure(c, cfg.inject_count);
+    g_injected = true;
+  }
+}
+
 static int check(const Config &cfg, uint32_t q, uint32_t fft_req, const std::string &aid) {
   const uint32_t end = (q + 31) / 32;
   const uint32_t last = q - 2;
@@ -378,7 +438,8 @@ static int check(const Config &cfg, uint32_t q, uint32_t fft_req, const std::str
     Run r;
     r.q = q;
     r.n = n;
-    ll_status s = ll_create(cfg.device, q, n, nullptr, &r.ctx);
+    ll_tuning tu{};
+    ll_status s = ll_create(cfg.device, q, n, shape_for(cfg, n, tu) ? &tu : nullptr, &r.ctx);
     if (s != LL_OK) { fail(nullptr, s, "ll_create"); return 2; }
     digits.assign(n, 0);
     if (fresh) {
@@ -393,19 +454,44 @@ static int check(const Config &cfg, uint32_t q, uint32_t fft_req, const std::str
     }
     if (s != LL_OK) { fail(r.ctx, s, "start"); return 2; }
     fflush(stdout);
+    if (fresh && j == 1 && cfg.roundoff_test) {
+      const int rt = round_off_test(r.ctx, q, n, j, offset);
+      if (rt < 0) return 2;
+      if (rt > 0) {
+        const uint32_t nn = next_length(q, n);
+        if (!nn) { printf("Something is wrong! Quitting.\n\n"); return 2; }
+        n = nn;
+        continue;  // a fresh start at the longer length
+      }
+      // the state after the round-off test is the first restart point
+      s = ll_read_digits(r.ctx, digits.data(), &offset);
+      if (s != LL_OK) { fail(r.ctx, s, "ll_read_digits"); return 2; }
+      std::vector<int32_t> std_d(digits);
+      ll_digits_standardize(std_d.data(), q, n);
+      ll_pack_bits(std_d.data(), state.data(), q, n);
+      state[end] = q;
+      state[end + 1] = n;
+      state[end + 2] = j;
+      state[end + 3] = offset;
+      fresh = false;
+    }
     uint32_t last_report = j - 1;
     double t0 = now_s();
     float maxerr = 0.f;
     bool restart = false;
+    // error read-back every 100 iterations (CUDALucas.cu:2936), or every
+    // PoliteValue iterations in polite mode (CUDALucas.cu:1979)
+    const uint32_t chunk = cfg.polite && cfg.polite_value > 0 && cfg.polite_value < 100 ? cfg.polite_value : 100;
     while (j <= last) {
-      // advance to the next multiple of 100, report or checkpoint boundary
-      uint32_t stop = (j / 100 + 1) * 100;
+      // advance to the next multiple of the chunk, report or checkpoint boundary
+      uint32_t stop = (j / chunk + 1) * chunk;
       const uint32_t rep = (j / cfg.report_iters + 1) * cfg.report_iters;
       if (rep < stop) stop = rep;
       if (stop > last) stop = last;
       if (stop < j) stop = j;
       const bool report = (stop % cfg.report_iters == 0) || stop == last || g_quit;
       float err = 0.f;
+      maybe_inject(cfg, r.ctx, j);
       s = ll_step(r.ctx, stop - j + 1, report ? LL_REPORT : LL_ERRCHK, &err);
       if (s != LL_OK) {
         fail(r.ctx, s, "ll_step");
@@ -522,9 +608,9 @@ static int check(const Config &cfg, uint32_t q, uint32_t fft_req, const std::str
 }
 
 // ------------------------------------------------------------- self-test --
-// Res64 of s_10000 (s0 = 4) for the reference's self-test exponents
-// (CUDALucas.cu:2673-2729); loaded from the same JSON the tests use when
-// present, otherwise the short table below is used.
+// Res64 of s_10000 (s0 = 4) for the reference's self-test exponents: the
+// short table (-r 0, CUDALucas.cu:2673-2682) and the long one (-r 1,
+// CUDALucas.cu:2684-2729), kept as the known answers.
 struct Kat { uint32_t p; uint64_t r; };
 static const Kat kShort[] = {
     {86243, 0x23992ccd735a03d9ull},   {132049, 0x4c52a92b54635f9eull},  {216091, 0x30247786758b8792ull},
@@ -534,35 +620,215 @@ static const Kat kShort[] = {
     {24036583, 0xcbdef38a0bdc4f00ull}, {25964951, 0x62eb3ff0a5f6237cull}, {30402457, 0x0b8600ef47e69d27ull},
     {32582657, 0x02751b7fcec76bb1ull}, {37156667, 0x67ad7646a1fad514ull}, {42643801, 0x8f90d78d5007bba7ull},
     {43112609, 0xe86891ebf6cd70c4ull}, {57885161, 0x76c27556683cd84dull}};
+static const Kat kLong[] = {
+    {22133, 0xb3ed67a5d4be2a9full}, {43633, 0xa3f3e669e061bfbeull}, {85933, 0x474e01b06d9698f8ull},
+    {169409, 0x3d32414583ac7d9aull}, {190097, 0xf681a2a2ad0397fbull}, {210739, 0x7e3b5a8b4e4c43a0ull},
+    {292921, 0xade86fd9a4ad99f1ull}, {333803, 0xe7311b6b953a609full}, {374587, 0xdb4ca1fad1c3e276ull},
+    {435571, 0xb6711834a5dd0ad1ull}, {657719, 0xc56715170d6819efull}, {738083, 0x2d6f637091a3ce6dull},
+    {818239, 0xe63f1cc63af264cbull}, {978041, 0xc049101d2a0f945bull}, {1137271, 0x8e006ecd6719158full},
+    {1216693, 0x847bbf5d0a077cadull}, {1296011, 0xc5002ae321cc3055ull}, {1414741, 0x7c6237b4f067d8caull},
+    {1612249, 0xfd4c832d1dbf746full}, {1927129, 0x155eb42707e90cd9ull}, {2240863, 0xf5e629fcc1247e4aull},
+    {2397383, 0xf58df7be5d73b369ull}, {2553659, 0x0a9357c955a13ca5ull}, {2865601, 0xdac4555e41809026ull},
+    {3176779, 0x1a8ed18fa285f151ull}, {3215629, 0x9e0c8eb95b15ae66ull}, {3332107, 0x7a539a9b8060b0d8ull},
+    {3564823, 0x820e428ad972cd86ull}, {3797219, 0xa7223e4ecad04860ull}, {3874583, 0xf60c0a837ec80a50ull},
+    {3951977, 0xb5da72b662eb3652ull}, {4415431, 0x31d58de3e1d79a85ull}, {4723783, 0x89fac94192cc3becull},
+    {5031737, 0x6371a0f4aef2af32ull}, {5646379, 0xf03d3bbaa51fbe63ull}, {6259537, 0x026805e6b4f1b0feull},
+    {6336103, 0x0f0718d2da4aaad3ull}, {6565633, 0x98d84929de4e6f63ull}, {7024163, 0xc030210791a14e9cull},
+    {7482053, 0xf54842c06ba7e3c4ull}, {7634537, 0x24872a305faae4f8ull}, {7786967, 0x060dfca872385f9bull},
+    {8700169, 0x4f95b9afd65b3c7eull}, {9914521, 0xc6ff39fd699d624cull}, {11125619, 0x1484b22a17312da0ull},
+    {12333809, 0xbd8435b83f062d6aull}, {12484649, 0xd56aa903718b2353ull}, {12936919, 0x1527f970ad3020bfull},
+    {13840423, 0x002a2aa0b97306b7ull}, {14742617, 0xf63addc70cde0addull}, {15043099, 0xe52f5e2045a2db30ull},
+    {15343429, 0x5eda3ab1816505b9ull}, {16543493, 0x85ea99f94dc20a8bull}, {17142793, 0x94edb737270e4ca7ull},
+    {17217653, 0x3ec0aa4728b97ef3ull}, {19535569, 0x708d03d1fe4c06f2ull}, {21921901, 0x38651890258c09bbull},
+    {22368691, 0xcc264d5bc61bc957ull}, {24599717, 0x76e7ab92aca768abull}, {25490893, 0x135f7e63e7357efbull},
+    {27271147, 0xb1a47be0366530efull}, {29640913, 0x4d51f44ffae1c913ull}, {30232693, 0xcab02c7178561218ull},
+    {32597297, 0xec15163c817fcfddull}, {33778141, 0x9145db2f2080172eull}, {38492887, 0x36efe22824adb35cull},
+    {43194913, 0xf13bdac634316fa2ull}, {47885689, 0x51a71b010cacfd92ull}, {48471289, 0x5f504f82abefdd1cull},
+    {50227213, 0x643739d94fe6789cull}, {53735041, 0x653267115ab57688ull}, {58404433, 0x6e4b3224349080c8ull},
+    {59570449, 0x8d7c6550107a2d0aull}, {64229677, 0x796701d5562dce22ull}, {66556463, 0xe418b5d4fb5c7e45ull},
+    {66847171, 0xc01ffc681dbb8966ull}, {75846319, 0x626ab6b09b607ba9ull}, {85111207, 0x14bb68062d100ebdull},
+    {86845813, 0x88220ac98093b65cull}, {95507747, 0xa92c24ad9b6655f1ull}, {97454309, 0xd6d4b3b14c1b73d8ull},
+    {105879517, 0x3310a4b03a18f4a8ull}, {111056879, 0x59e95ddb73c59624ull}, {115080019, 0x293d0b202c9e3c63ull},
+    {117377567, 0xdf57cd5d866f1065ull}, {118813021, 0x1cd6a8caef092277ull}, {126558077, 0x40b1cf42af7f99a7ull},
+    {131142761, 0x046ab21b10a27189ull}, {131715607, 0x8fcfb36b868738ecull}, {142017539, 0x801794367f35ccb6ull},
+    {147162241, 0x72c8773764a260b0ull}, {149447533, 0x24702427a0f5d673ull},
+};
 
+// check_residue (CUDALucas.cu:2731-2805): 10000 iterations of each table
+// exponent at its default length, with the round-off test first when
+// RoundoffTest is set; an iteration error above 0.4 moves to the next
+// length and restarts the exponent.
 static int selftest(const Config &cfg) {
   int bad = 0;
-  for (const Kat &k : kShort) {
-    const uint32_t n = ll_choose_fft_length(k.p, 0);
-    ll_ctx *c = nullptr;
-    ll_status s = ll_create(cfg.device, k.p, n, nullptr, &c);
-    if (s != LL_OK) { fail(nullptr, s, "ll_create"); return 2; }
-    printf("Starting self test M%u fft length = %uK\n", k.p, n / 1024);
-    const double t0 = now_s();
-    float err = 0.f;
+  const Kat *tab = cfg.selftest ? kLong : kShort;
+  const size_t cnt = cfg.selftest ? sizeof(kLong) / sizeof(kLong[0]) : sizeof(kShort) / sizeof(kShort[0]);
+  const uint32_t last = 10000;
+  for (size_t t = 0; t < cnt; ++t) {
+    const Kat &k = tab[t];
+    uint32_t n = ll_choose_fft_length(k.p, 0);
     uint64_t r = 0;
-    s = ll_start(c, (uint32_t)(rand() % k.p));
-    if (s == LL_OK) s = ll_step(c, 10000, LL_REPORT, &err);
-    if (s == LL_OK) s = ll_res64(c, &r);
-    const double dt = now_s() - t0;
-    if (s != LL_OK) { fail(c, s, "self test"); ll_destroy(c); return 2; }
-    printf("Iteration 10000 / %u, 0x%016llx, %uK, %s, error = %5.5f, real: %s, %4.4f ms/iter\n", k.p,
-           (unsigned long long)r, n / 1024, kProgram, err, fmt_time((unsigned)dt).c_str(), dt * 1000.0 / 10000);
+    float maxerr = 0.f;
+    double dt = 0.0;
+    bool restarting;
+    bool first = true;
+    do {
+      restarting = false;
+      if (!n) { fprintf(stderr, "No usable FFT length for M%u\n", k.p); return 2; }
+      ll_ctx *c = nullptr;
+      ll_tuning tu{};
+      ll_status s = ll_create(cfg.device, k.p, n, shape_for(cfg, n, tu) ? &tu : nullptr, &c);
+      if (s != LL_OK) { fail(nullptr, s, "ll_create"); return 2; }
+      if (first) printf("Starting self test M%u fft length = %uK\n", k.p, n / 1024);
+      first = false;
+      const double t0 = now_s();
+      uint32_t j = 1, offset = (uint32_t)(rand() % k.p);
+      s = ll_start(c, offset);
+      if (s == LL_OK && cfg.roundoff_test) {
+        const int rt = round_off_test(c, k.p, n, j, offset);
+        if (rt < 0) { ll_destroy(c); return 2; }
+        if (rt > 0) restarting = true;
+      }
+      maxerr = 0.f;
+      while (s == LL_OK && !restarting && j <= last) {
+        const uint32_t stop = std::min<uint32_t>((j / 100 + 1) * 100, last);
+        float err = 0.f;
+        s = ll_step(c, stop - j + 1, stop == last ? LL_REPORT : LL_ERRCHK, &err);
+        if (err > maxerr) maxerr = err;
+        if (err > 0.4f) restarting = true;
+        j = stop + 1;
+      }
+      if (s == LL_OK && !restarting) s = ll_res64(c, &r);
+      if (s != LL_OK) { fail(c, s, "self test"); ll_destroy(c); return 2; }
+      ll_destroy(c);
+      dt = now_s() - t0;
+      if (restarting) n = next_length(k.p, n);
+    } while (restarting);
+    printf("Iteration %u / %u, 0x%016llx, %uK, %s, error = %5.5f, real: %s, %4.4f ms/iter\n", last, k.p,
+           (unsigned long long)r, n / 1024, kProgram, maxerr, fmt_time((unsigned)dt).c_str(), dt * 1000.0 / last);
     if (r != k.r) {
       printf("Expected residue [%016llx] does not match actual residue [%016llx]\n\n", (unsigned long long)k.r,
              (unsigned long long)r);
       ++bad;
     } else
       printf("This residue is correct.\n\n");
-    ll_destroy(c);
+    fflush(stdout);
   }
   if (bad) fprintf(stderr, "Error: There %s %d bad selftest%s!\n", bad > 1 ? "were" : "was", bad, bad > 1 ? "s" : "");
   return bad ? 1 : 0;
+}
+
+// ------------------------------------------------------------ fft.txt --
+// `<gpu> fft.txt` in the reference's layout (CUDALucas.cu:2555-2573): device
+// lines, a header, then one "%5d %10d %8.4f" row per kept length (length in
+// K, largest exponent, ms/iter).  init_ffts reads every line whose leading
+// number is non-zero as a length in K (CUDALucas.cu:975-990).
+static std::vector<uint32_t> read_fft_file(const std::string &name) {
+  std::vector<uint32_t> out;
+  FILE *f = fopen(name.c_str(), "r");
+  if (!f) return out;
+  char buf[192];
+  while (fgets(buf, sizeof buf, f)) {
+    const int k = atoi(buf);
+    if (k > 0) out.push_back((uint32_t)k * 1024u);
+  }
+  fclose(f);
+  std::sort(out.begin(), out.end());
+  out.erase(std::unique(out.begin(), out.end()), out.end());
+  return out;
+}
+
+// -cufftbench s e passes (CUDALucas.cu:2413-2587): times every supported
+// length from s K to e K (passes x 50 iterations after a warm-up of 50),
+// keeps the lengths faster than every longer one (and the powers of two),
+// writes them to `<gpu> fft.txt`, moving an older file aside as the
+// reference does.  For each length the fastest launch shape among the
+// engine's candidates (row width W) goes to `<gpu> shapes.txt`.
+static int cufftbench(const Config &cfg, const char *gpu, int s, int e, int passes) {
+  if (!gpu[0]) { fprintf(stderr, "no CUDA device %d\n", cfg.device); return 2; }
+  std::vector<uint32_t> lens;
+  std::vector<float> times;
+  std::vector<int32_t> widths;
+  for (int k = s; k <= e; ++k) {
+    const uint32_t n = (uint32_t)k * 1024u;
+    if (!ll_length_supported(n)) continue;
+    uint32_t q = (uint32_t)(n * 17.6) | 1;
+    while (!is_prime(q)) q += 2;
+    float best = 0.f;
+    int32_t best_w = 0;
+    // candidate row widths: the engine's own choice first, then the
+    // divisors of N = n/2 near its square root
+    std::vector<int32_t> cand = {0};
+    const uint32_t N = n / 2;
+    for (uint32_t w = 64; w <= 8192 && w <= N; w += 2)
+      if (N % w == 0 && (double)w * w >= N / 16.0 && (double)w * w <= 16.0 * N) cand.push_back((int32_t)w);
+    for (int32_t w : cand) {
+      ll_tuning tu{};
+      tu.width = w;
+      ll_ctx *c = nullptr;
+      if (ll_create(cfg.device, q, n, w ? &tu : nullptr, &c) != LL_OK) continue;
+      int32_t W = 0;
+      ll_shape(c, &W, nullptr, nullptr, nullptr, nullptr);
+      if (w && w != W) { ll_destroy(c); continue; }
+      float err = 0.f;
+      ll_start(c, 0);
+      ll_step(c, 50, LL_ERRCHK, &err);
+      const double t0 = now_s();
+      const ll_status st = ll_step(c, 50 * (uint32_t)passes, LL_ERRCHK, &err);
+      const float ms = (float)((now_s() - t0) * 1000.0 / (50.0 * passes));
+      ll_destroy(c);
+      if (st != LL_OK) continue;
+      if (best == 0.f || ms < best) { best = ms; best_w = W; }
+    }
+    if (best == 0.f) continue;
+    printf("fft size = %uK, ave time = %6.4f msec, width %d\n", n / 1024, best, best_w);
+    fflush(stdout);
+    lens.push_back(n);
+    times.push_back(best);
+    widths.push_back(best_w);
+  }
+  std::vector<int32_t> keep(lens.size(), 0);
+  ll_fft_prune(lens.data(), times.data(), (int32_t)lens.size(), keep.data());
+  const std::string name = std::string(gpu) + " fft.txt";
+  char stamp[64];
+  const time_t now = time(nullptr);
+  strftime(stamp, sizeof stamp, "%d%H%M%S", localtime(&now));
+  const std::string bak = std::string(gpu) + " fft" + stamp + ".txt";
+  unlink(bak.c_str());
+  rename(name.c_str(), bak.c_str());
+  FILE *f = fopen(name.c_str(), "w");
+  FILE *g = fopen((std::string(gpu) + " shapes.txt").c_str(), "w");
+  if (!f) { fprintf(stderr, "Cannot open %s.\n", name.c_str()); return 2; }
+  fprintf(f, "Device              %s\n\n  fft    max exp  ms/iter\n", gpu);
+  if (g) fprintf(g, "# fft(K) width ms/iter\n");
+  for (size_t i = 0; i < lens.size(); ++i) {
+    if (g) fprintf(g, "%5u %6d %8.4f\n", lens[i] / 1024, widths[i], times[i]);
+    if (keep[i]) fprintf(f, "%5u %10u %8.4f\n", lens[i] / 1024, ll_fft_max_exponent(lens[i]), times[i]);
+  }
+  fclose(f);
+  if (g) fclose(g);
+  printf("Old %s moved to %s.\nOptimal fft lengths saved in %s.\n", name.c_str(), bak.c_str(), name.c_str());
+  return 0;
+}
+
+// The launch shape measured fastest for length n (`<gpu> shapes.txt`), if any.
+static bool shape_for(const Config &cfg, uint32_t n, ll_tuning &tu) {
+  char gpu[256];
+  if (ll_device_name(cfg.device, gpu, sizeof gpu)) return false;
+  FILE *f = fopen((std::string(gpu) + " shapes.txt").c_str(), "r");
+  if (!f) return false;
+  char buf[192];
+  bool found = false;
+  while (fgets(buf, sizeof buf, f)) {
+    unsigned k = 0;
+    int w = 0;
+    if (buf[0] != '#' && sscanf(buf, "%u %d", &k, &w) == 2 && k * 1024u == n && w > 0) {
+      tu = ll_tuning{};
+      tu.width = w;
+      found = true;
+    }
+  }
+  fclose(f);
+  return found;
 }
 
 // ------------------------------------------------------------------ main --
@@ -648,29 +914,25 @@ int main(int argc, char **argv) {
   }
   cfg.report_iters = check_interval(cfg.report_iters);
   cfg.check_iters = check_interval(cfg.check_iters);
-  if (cfg.selftest >= 0) return selftest(cfg);
-  if (bench_p > 0) {
-    // time table lengths in [s, e] K: passes x 50 iterations each
-    std::vector<uint32_t> t(256);
-    int cnt = ll_fft_table(t.data(), (int)t.size());
-    for (int i = 0; i < cnt; ++i) {
-      uint32_t n = t[i];
-      if (n < (uint32_t)bench_s * 1024 || n > (uint32_t)bench_e * 1024 || !ll_length_supported(n)) continue;
-      uint32_t q = (uint32_t)(n * 17.6) | 1;
-      while (!is_prime(q)) q += 2;
-      ll_ctx *c = nullptr;
-      if (ll_create(cfg.device, q, n, nullptr, &c) != LL_OK) continue;
-      ll_start(c, 0);
-      float err;
-      ll_step(c, 50, LL_ERRCHK, &err);
-      double t0 = now_s();
-      ll_step(c, 50 * (uint32_t)bench_p, LL_ERRCHK, &err);
-      double ms = (now_s() - t0) * 1000.0 / (50.0 * bench_p);
-      printf("fft size = %uK, ave time = %2.4f msec\n", n / 1024, ms);
-      ll_destroy(c);
+  if (const char *inj = getenv("LLUCAS_INJECT_FAILURES")) {
+    unsigned at = 0;
+    int cnt = 0;
+    if (sscanf(inj, "%u:%d", &at, &cnt) == 2) {
+      cfg.inject_at = at;
+      cfg.inject_count = cnt;
     }
-    return 0;
   }
+  char gpu[256] = "";
+  const bool have_gpu = ll_device_name(cfg.device, gpu, sizeof gpu) == 0;
+  if (bench_p > 0) return cufftbench(cfg, gpu, bench_s, bench_e, bench_p);
+  // init_ffts (CUDALucas.cu:975-1021): a `<gpu> fft.txt` written by an
+  // earlier -cufftbench restricts the lengths inside its range to the
+  // measured ones
+  if (have_gpu) {
+    const std::vector<uint32_t> measured = read_fft_file(std::string(gpu) + " fft.txt");
+    if (!measured.empty()) ll_fft_table_merge(measured.data(), (int32_t)measured.size());
+  }
+  if (cfg.selftest >= 0) return selftest(cfg);
   if (target.empty()) target = cfg.workfile;
   char *endp = nullptr;
   unsigned long q = strtoul(target.c_str(), &endp, 10);

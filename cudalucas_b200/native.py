@@ -19,6 +19,7 @@ LL_ERR_TIMEOUT = 6
 LL_ERR_INJECTED = 7
 LL_REPORT = 1
 LL_ERRCHK = 2
+LL_ASYNC = 4
 LL_STATIC_MAX_WORDS = 1 << 20
 
 
@@ -82,6 +83,10 @@ def lib():
         "ll_choose_fft_length": (u32, [u32, u32]),
         "ll_fft_table": (i32, [u32p, i32]),
         "ll_length_supported": (i32, [u32]),
+        "ll_fft_table_merge": (i32, [u32p, i32]),
+        "ll_fft_prune": (i32, [u32p, ctypes.POINTER(ctypes.c_float), i32, i32p]),
+        "ll_fft_max_exponent": (u32, [u32]),
+        "ll_device_name": (i32, [ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(L, name)

@@ -38,6 +38,11 @@ typedef enum {
  * mirrors bit 1 (max roundoff error read back, CUDALucas.cu:1973-1978). */
 #define LL_REPORT 1u
 #define LL_ERRCHK 2u
+/* LL_ASYNC: only enqueue, even with LL_REPORT or LL_ERRCHK.  With LL_REPORT
+ * the digits become readable once the stream has finished (ll_read_digits
+ * waits for it); the roundoff maximum keeps accumulating on the device until
+ * the next call that reads it back. */
+#define LL_ASYNC 4u
 
 typedef struct ll_ctx ll_ctx;
 
@@ -71,9 +76,9 @@ ll_status ll_load_digits(ll_ctx *ctx, const int32_t *digits, uint32_t offset);
 
 /* Runs `iters` LL iterations (iters x lucas_square, CUDALucas.cu:1869).
  * LL_REPORT: digits of the final state become readable by ll_read_digits.
- * LL_REPORT or LL_ERRCHK: waits for the GPU and stores the max roundoff
- * error seen since the last read in *max_err (may be NULL).  Without either
- * flag the call only enqueues work and returns. */
+ * LL_REPORT or LL_ERRCHK (without LL_ASYNC): waits for the GPU and stores
+ * the max roundoff error seen since the last read in *max_err (may be NULL).
+ * Without either flag, or with LL_ASYNC, the call only enqueues work. */
 ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err);
 
 /* Copies the n digits written by the last LL_REPORT step (or the last
@@ -139,15 +144,17 @@ ll_status ll_batch_res64(ll_batch *b, uint64_t *res64);
  * It reads n balanced digits of x = s*2^offset from DEVICE memory digits_in,
  * runs `iters` LL iterations and writes the digits of the result (whose
  * offset is offset*2^iters mod q) to DEVICE memory digits_out; the max
- * roundoff error goes to the HOST float *max_err (may be NULL).  All scratch
+ * roundoff error goes to the HOST float *max_err (may be NULL), as 1.0 when a
+ * word left the exact FP64 range (the digits are then invalid).  All scratch
  * lives in one static array of LL_STATIC_SCRATCH_BYTES per device (held by
  * every GPU that loads the library, until exit); n may not exceed
  * LL_STATIC_MAX_WORDS (LL_ERR_ARG otherwise).  The first call on a device
  * looks up the array's device address; make that call before any stream
- * capture.  Calls share the array: calls that overlap on the GPU (other
- * streams, other host threads' GPU work still running) race.  The call
- * synchronises `stream` (a cudaStream_t, NULL = legacy default stream) before
- * it returns. */
+ * capture.  Calls share the array and it keeps the last call's contents:
+ * calls whose GPU work overlapped would race.  Each call therefore holds a
+ * lock of its device until its work has finished: it synchronises `stream`
+ * (a cudaStream_t, NULL = legacy default stream) before it returns, also on
+ * an error, and calls on different devices do not wait for each other. */
 #define LL_STATIC_MAX_WORDS (1u << 20)
 #define LL_STATIC_SCRATCH_BYTES (16u << 20)
 ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t offset, uint32_t iters,
@@ -187,6 +194,29 @@ void ll_fft_bounds(uint32_t q, uint32_t *lb, uint32_t *ub);
 uint32_t ll_choose_fft_length(uint32_t q, uint32_t want);
 int32_t ll_fft_table(uint32_t *lengths, int32_t max_count);
 int32_t ll_length_supported(uint32_t n);
+
+/* init_ffts (CUDALucas.cu:947-1022) with a `<gpu> fft.txt` present: installs,
+ * process-wide, the table made of the built-in lengths below the smallest
+ * measured length, the measured lengths, and the built-in lengths above the
+ * largest one, so that ll_choose_fft_length and ll_fft_table skip lengths the
+ * benchmark found slower than a longer length.  `measured` is ascending (the
+ * benchmark's list, in words); count 0 restores the built-in table.  Returns
+ * the new table's size, -1 on a bad argument. */
+int32_t ll_fft_table_merge(const uint32_t *measured, int32_t count);
+
+/* The pruning rule of -cufftbench (CUDALucas.cu:2500-2513) over lengths in
+ * ascending order with their measured ms/iter: keep[i] = 1 when length i is
+ * faster than every longer length, or is a power of two in K.  Returns the
+ * number kept, -1 on a bad argument. */
+int32_t ll_fft_prune(const uint32_t *lengths, const float *ms_per_iter, int32_t count, int32_t *keep);
+
+/* The largest exponent whose lower length bound (ll_fft_bounds) is <= n:
+ * the `max exp` column of `<gpu> fft.txt`. */
+uint32_t ll_fft_max_exponent(uint32_t n);
+
+/* Name of CUDA device `device` (for the per-GPU `<gpu> fft.txt` and
+ * `<gpu> shapes.txt` files); returns 0 on success. */
+int32_t ll_device_name(int device, char *name, size_t len);
 
 #ifdef __cplusplus
 }

@@ -41,6 +41,8 @@ def lib():
         L.oracle_checkpoint_checksum.argtypes = [ctypes.c_char_p, i]
         L.oracle_ch_sum.restype = ctypes.c_uint
         L.oracle_ch_sum.argtypes = [up, i]
+        L.oracle_set_threads.restype = i
+        L.oracle_set_threads.argtypes = [i]
         _lib = L
     return _lib
 
@@ -51,6 +53,11 @@ def _ip(a):
 
 def _up(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint))
+
+
+def set_threads(t):
+    """Host threads of the oracle's parallel loops; returns the count in effect."""
+    return lib().oracle_set_threads(int(t))
 
 
 class Oracle:

@@ -1,9 +1,12 @@
 /*
  * ORACLE — test infrastructure only.
  *
- * A plain-C, single-threaded CPU restatement of the Lucas-Lehmer squaring
- * step of CUDALucas v2.06 (IBDWT in FP64), used as the checker for the CUDA
- * engine and as the timed host-core baseline.  Only tests/, the smoke check
+ * A plain-C CPU restatement of the Lucas-Lehmer squaring step of CUDALucas
+ * v2.06 (IBDWT in FP64), used as the checker for the CUDA engine and as the
+ * timed host-core baseline.  The loops over independent butterflies, pairs
+ * and carry blocks can be split over several host threads
+ * (oracle_set_threads, POSIX threads); every output word is computed by the
+ * same arithmetic whatever the thread count, so results do not depend on it.  Only tests/, the smoke check
  * and bench.py's cpu_baseline leg may load it; the product never does.
  *
  * Each function names the reference code it follows (file:line within the
@@ -19,11 +22,43 @@
  * against exact big-integer arithmetic (oracle/exact.py).
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
 typedef struct { double re, im; } cplx;
+
+/* ------------------------------------------------------ host threads -- */
+/* par_for(count, fn, arg): fn(arg, lo, hi, slot) over [0, count) split into
+ * contiguous ranges, one per thread (slot = range index < g_threads). */
+#define ORACLE_MAX_THREADS 256
+static int g_threads = 1;
+typedef void (*range_fn)(void *arg, int lo, int hi, int slot);
+typedef struct { range_fn fn; void *arg; int lo, hi, slot; } par_job;
+
+static void *par_run(void *p) {
+  par_job *j = (par_job *)p;
+  j->fn(j->arg, j->lo, j->hi, j->slot);
+  return NULL;
+}
+
+static void par_for(int count, range_fn fn, void *arg) {
+  int t = g_threads < count ? g_threads : count;
+  if (t <= 1) { fn(arg, 0, count, 0); return; }
+  pthread_t th[ORACLE_MAX_THREADS];
+  par_job jobs[ORACLE_MAX_THREADS];
+  int started[ORACLE_MAX_THREADS];
+  for (int i = 0; i < t; i++) {
+    jobs[i].fn = fn; jobs[i].arg = arg; jobs[i].slot = i;
+    jobs[i].lo = (int)((long long)count * i / t);
+    jobs[i].hi = (int)((long long)count * (i + 1) / t);
+    started[i] = i > 0 && pthread_create(&th[i], NULL, par_run, &jobs[i]) == 0;
+    if (i > 0 && !started[i]) par_run(&jobs[i]);  /* no thread: run it here */
+  }
+  par_run(&jobs[0]);
+  for (int i = 1; i < t; i++) if (started[i]) pthread_join(th[i], NULL);
+}
 
 /* ------------------------------------------------------------------ FFT -- */
 /* Mixed-radix Stockham FFT, exponent sign +1 (cuFFT's CUFFT_INVERSE),
@@ -67,46 +102,58 @@ static inline cplx cmul(cplx a, cplx b) {
   return r;
 }
 
+/* one Stockham stage: butterflies j in [lo, hi) */
+typedef struct { const fft_plan *p; const cplx *in; cplx *out; int R, m, ns; } fft_stage;
+
+static void fft_stage_range(void *arg, int lo, int hi, int slot) {
+  const fft_stage *st = (const fft_stage *)arg;
+  const fft_plan *p = st->p;
+  const int L = p->len, R = st->R, m = st->m, ns = st->ns;
+  const cplx *in = st->in;
+  cplx *out = st->out;
+  cplx v[7], w[7];
+  (void)slot;
+  for (int j = lo; j < hi; j++) {
+    int k = j % ns;
+    for (int r = 0; r < R; r++) {
+      v[r] = in[j + r * m];
+      if (r && k) v[r] = cmul(v[r], p->tw[(size_t)r * k * (L / (ns * R)) % L]);
+    }
+    if (R == 2) {
+      w[0].re = v[0].re + v[1].re; w[0].im = v[0].im + v[1].im;
+      w[1].re = v[0].re - v[1].re; w[1].im = v[0].im - v[1].im;
+    } else if (R == 4) {
+      /* sign +1: multiply by +i on the odd difference */
+      cplx s0 = {v[0].re + v[2].re, v[0].im + v[2].im}, d0 = {v[0].re - v[2].re, v[0].im - v[2].im};
+      cplx s1 = {v[1].re + v[3].re, v[1].im + v[3].im}, d1 = {v[1].re - v[3].re, v[1].im - v[3].im};
+      w[0].re = s0.re + s1.re; w[0].im = s0.im + s1.im;
+      w[2].re = s0.re - s1.re; w[2].im = s0.im - s1.im;
+      w[1].re = d0.re - d1.im; w[1].im = d0.im + d1.re;
+      w[3].re = d0.re + d1.im; w[3].im = d0.im - d1.re;
+    } else {
+      /* direct DFT_R for the odd radices 3, 5, 7 */
+      for (int a = 0; a < R; a++) {
+        cplx acc = v[0];
+        for (int c = 1; c < R; c++) {
+          cplx t = cmul(v[c], p->tw[(size_t)((a * c) % R) * (L / R)]);
+          acc.re += t.re; acc.im += t.im;
+        }
+        w[a] = acc;
+      }
+    }
+    int base = (j / ns) * ns * R + k;
+    for (int r = 0; r < R; r++) out[base + r * ns] = w[r];
+  }
+}
+
 /* in-place, sign +1 */
 static void fft_exec(fft_plan *p, cplx *x) {
   int L = p->len, ns = 1;
   cplx *in = x, *out = p->tmp;
-  cplx v[7], w[7];
   for (int s = 0; s < p->nst; s++) {
-    int R = p->radix[s];
-    int m = L / R;
-    for (int j = 0; j < m; j++) {
-      int k = j % ns;
-      for (int r = 0; r < R; r++) {
-        v[r] = in[j + r * m];
-        if (r && k) v[r] = cmul(v[r], p->tw[(size_t)r * k * (L / (ns * R)) % L]);
-      }
-      if (R == 2) {
-        w[0].re = v[0].re + v[1].re; w[0].im = v[0].im + v[1].im;
-        w[1].re = v[0].re - v[1].re; w[1].im = v[0].im - v[1].im;
-      } else if (R == 4) {
-        /* sign +1: multiply by +i on the odd difference */
-        cplx s0 = {v[0].re + v[2].re, v[0].im + v[2].im}, d0 = {v[0].re - v[2].re, v[0].im - v[2].im};
-        cplx s1 = {v[1].re + v[3].re, v[1].im + v[3].im}, d1 = {v[1].re - v[3].re, v[1].im - v[3].im};
-        w[0].re = s0.re + s1.re; w[0].im = s0.im + s1.im;
-        w[2].re = s0.re - s1.re; w[2].im = s0.im - s1.im;
-        w[1].re = d0.re - d1.im; w[1].im = d0.im + d1.re;
-        w[3].re = d0.re + d1.im; w[3].im = d0.im - d1.re;
-      } else {
-        /* direct DFT_R for the odd radices 3, 5, 7 */
-        for (int a = 0; a < R; a++) {
-          cplx acc = v[0];
-          for (int c = 1; c < R; c++) {
-            cplx t = cmul(v[c], p->tw[(size_t)((a * c) % R) * (L / R)]);
-            acc.re += t.re; acc.im += t.im;
-          }
-          w[a] = acc;
-        }
-      }
-      int base = (j / ns) * ns * R + k;
-      for (int r = 0; r < R; r++) out[base + r * ns] = w[r];
-    }
-    ns *= R;
+    fft_stage st = {p, in, out, p->radix[s], L / p->radix[s], ns};
+    par_for(st.m, fft_stage_range, &st);
+    ns *= st.R;
     cplx *t = in; in = out; out = t;
   }
   if (in != x) memcpy(x, in, sizeof(cplx) * (size_t)L);
@@ -237,13 +284,23 @@ void oracle_destroy(oracle_ctx *c) {
 }
 
 /* apply_weights, CUDALucas.cu:216-249 */
-static void apply_weights(oracle_ctx *c, const int *in) {
-  for (int idx = 0; idx < c->n; idx++) {
+typedef struct { oracle_ctx *c; const int *in; } weights_job;
+
+static void apply_weights_range(void *arg, int lo, int hi, int slot) {
+  oracle_ctx *c = ((weights_job *)arg)->c;
+  const int *in = ((weights_job *)arg)->in;
+  (void)slot;
+  for (int idx = lo; idx < hi; idx++) {
     int grp = idx >> 5, col = idx & 31;
     double tc = c->ttp[col << 1];
     if (c->s[grp * 2 + 1] & (1u << col)) tc *= 0.5;
     c->x[idx] = (double)in[idx] * c->ttp[grp * 2 + 64] * tc;
   }
+}
+
+static void apply_weights(oracle_ctx *c, const int *in) {
+  weights_job job = {c, in};
+  par_for(c->n, apply_weights_range, &job);
 }
 
 /* init_x, CUDALucas.cu:1254-1278, with the offset supplied by the caller
@@ -265,10 +322,13 @@ void oracle_init(oracle_ctx *c, const int *digits, int offset) {
 }
 
 /* square, CUDALucas.cu:255-314 */
-static void square(oracle_ctx *c) {
+static void square_range(void *arg, int lo, int hi, int slot) {
+  oracle_ctx *c = (oracle_ctx *)arg;
   int n = c->n, nc0 = n >> 2;
   double *a = c->x, *ct = c->ct;
-  for (int jj = 0; jj < nc0; jj++) {
+  (void)slot;
+  /* pair jj touches words 2jj, 2jj+1, n-2jj, n-2jj+1 only: independent */
+  for (int jj = lo; jj < hi; jj++) {
     int j = jj, nc;
     double wkr, wki, xr, xi, yr, aj, aj1, ak, ak1;
     if (j) {
@@ -308,14 +368,28 @@ static void square(oracle_ctx *c) {
   }
 }
 
+static void square(oracle_ctx *c) { par_for(c->n >> 2, square_range, c); }
+
 /* rcb / rcbl, CUDALucas.cu:322-484 and :536-679.  The 128-thread block is
  * simulated one row of 128 words at a time; `wide` selects the 64-bit carry
  * arithmetic of rcbl, otherwise carries are truncated to int as in rcb. */
-static void rcb(oracle_ctx *c, int report, int digit, int bit) {
+typedef struct {
+  oracle_ctx *c;
+  int report, digit, bit;
+  float err[ORACLE_MAX_THREADS];
+} rcb_job;
+
+/* the blocks are independent: each writes its own words and its own
+ * outgoing carry, which splice applies afterwards */
+static void rcb_range(void *arg, int lo, int hi, int slot) {
+  rcb_job *job = (rcb_job *)arg;
+  oracle_ctx *c = job->c;
+  const int report = job->report, digit = job->digit, bit = job->bit;
   const int TT = 128;
-  int n = c->n, sc = c->sc, nblk = n >> sc;
+  int sc = c->sc, nblk = c->n >> sc;
   long long carry[257];
-  for (int blk = 0; blk < nblk; blk++) {
+  float err = 0;
+  for (int blk = lo; blk < hi; blk++) {
     long long cfns = 0;
     float ferr_max = 0;
     for (int row = 0; row < (1 << sc) / TT; row++) {
@@ -379,15 +453,30 @@ static void rcb(oracle_ctx *c, int report, int digit, int bit) {
         if (row == 0 && t < 2) c->data[(blk << 1) + t] = (int)val[t];
       }
     }
-    if (ferr_max > c->err) c->err = ferr_max;
+    if (ferr_max > err) err = ferr_max;
     c->carry[(blk + 1) % nblk] = c->bigcarry ? cfns : (long long)(int)cfns;
   }
+  job->err[slot] = err;
+}
+
+static void rcb(oracle_ctx *c, int report, int digit, int bit) {
+  rcb_job job;
+  job.c = c; job.report = report; job.digit = digit; job.bit = bit;
+  for (int i = 0; i < ORACLE_MAX_THREADS; i++) job.err[i] = 0;
+  par_for(c->n >> c->sc, rcb_range, &job);
+  for (int i = 0; i < ORACLE_MAX_THREADS; i++)
+    if (job.err[i] > c->err) c->err = job.err[i];
 }
 
 /* splice / splicel, CUDALucas.cu:486-534 and :681-721 */
-static void splice(oracle_ctx *c, int report) {
-  int n = c->n, bw = 1 << c->sc, nblk = n / bw;
-  for (int blk = 0; blk < nblk; blk++) {
+typedef struct { oracle_ctx *c; int report; } splice_job;
+
+static void splice_range(void *arg, int lo, int hi, int slot) {
+  oracle_ctx *c = ((splice_job *)arg)->c;
+  const int report = ((splice_job *)arg)->report;
+  int bw = 1 << c->sc;
+  (void)slot;
+  for (int blk = lo; blk < hi; blk++) {
     int j = blk * bw;
     int numbits = c->qn;
     double temp = c->ttp1[blk];
@@ -406,6 +495,11 @@ static void splice(oracle_ctx *c, int report) {
     c->x[j + 1] = (double)t1 * temp;
     if (report) { c->xint[j] = (int)t0; c->xint[j + 1] = (int)t1; }
   }
+}
+
+static void splice(oracle_ctx *c, int report) {
+  splice_job job = {c, report};
+  par_for(c->n >> c->sc, splice_range, &job);
 }
 
 /* lucas_square, CUDALucas.cu:1869-1986 */
@@ -430,6 +524,13 @@ float oracle_step(oracle_ctx *c, int iters, int report_last) {
   c->err = 0;
   for (int i = 0; i < iters; i++) e = oracle_square(c, report_last && i == iters - 1);
   return e;
+}
+
+/* Host threads for the parallel loops (1 = the plain single-threaded run);
+ * returns the count in effect. */
+int oracle_set_threads(int t) {
+  if (t >= 1) g_threads = t < ORACLE_MAX_THREADS ? t : ORACLE_MAX_THREADS;
+  return g_threads;
 }
 
 void oracle_digits(const oracle_ctx *c, int *out) { memcpy(out, c->xint, sizeof(int) * (size_t)c->n); }

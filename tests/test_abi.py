@@ -120,3 +120,46 @@ def test_create_fails_cleanly_without_gpu_or_bad_args():
         cl.LLContext(4, 1024)          # q <= n
     with pytest.raises(cl.LLError):
         cl.LLContext(216091, 1000)     # n not a multiple of 4 of a smooth length
+
+
+def test_cufftbench_pruning_rule():
+    """CUDALucas.cu:2500-2513: from the longest length down, a length stays
+    when it is faster than every longer one; powers of two (in K) stay."""
+    K = 1024
+    lens = [2048 * K, 2880 * K, 3024 * K, 3136 * K, 3200 * K, 3584 * K]
+    ms = [0.050, 0.058, 0.065, 0.0998, 0.062, 0.070]
+    keep = cl.fft_prune(lens, ms)
+    assert keep == [True, True, False, False, True, True]
+    # a power of two slower than a longer length is still kept
+    assert cl.fft_prune([4096 * K, 4320 * K], [0.09, 0.08]) == [True, True]
+    assert cl.fft_prune([4000 * K, 4320 * K], [0.09, 0.08]) == [False, True]
+
+
+def test_measured_table_replaces_builtin_lengths_in_its_range():
+    """init_ffts with a `<gpu> fft.txt` (CUDALucas.cu:975-1021): inside the
+    measured range only measured lengths remain, so an exponent whose
+    default length (3136K for M57885161) measured slower than 3200K gets
+    3200K; outside the range the built-in lengths stay."""
+    K = 1024
+    lens = [2880 * K, 3024 * K, 3136 * K, 3200 * K, 3584 * K]
+    ms = [0.058, 0.065, 0.0998, 0.062, 0.070]
+    kept = [n for n, k in zip(lens, cl.fft_prune(lens, ms)) if k]
+    try:
+        size = cl.fft_table_merge(kept)
+        table = cl.fft_table()
+        assert size == len(table)
+        assert 3136 * K not in table and 3200 * K in table
+        assert cl.choose_fft_length(57885161) == 3200 * K
+        assert cl.choose_fft_length(216091) == 14 * K          # below the measured range
+        assert cl.choose_fft_length(332192831) == 19208 * K    # above it
+        assert table == sorted(table)
+    finally:
+        cl.fft_table_merge([])
+    assert cl.choose_fft_length(57885161) == 3136 * K
+    assert len(cl.fft_table()) == 162
+
+
+def test_fft_max_exponent_inverts_the_lower_bound():
+    for n in (12288, 3276800, 18874368):
+        q = cl.fft_max_exponent(n)
+        assert cl.fft_bounds(q)[0] <= n < cl.fft_bounds(q + 1)[0]

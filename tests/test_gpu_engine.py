@@ -191,8 +191,9 @@ def test_independent_contexts_interleaved():
         a.step(200)
         b.step(200)
     a.step(0, report=True)
-    ra = a.step(1, report=True) and a.res64()
-    rb = b.step(1, report=True) and b.res64()
+    a.step(1, report=True)
+    b.step(1, report=True)
+    ra, rb = a.res64(), b.res64()
     a.close()
     b.close()
     assert ra == exact.res64(86243, 1001)
@@ -216,3 +217,14 @@ def test_read_digits_requires_report():
         c.step(5)
         with pytest.raises(cl.LLError):
             c.read_digits()
+
+
+@pytest.mark.parametrize("q,n", [(86243, 4096), (216091, 12288), (1257787, 65536)])
+def test_words_beyond_fp64_range_report_max_error(q, n):
+    """Digits far outside the balanced range push the squared words beyond
+    2^51, where the roundoff reading has no fraction bits left; the wide pass
+    flags it and ll_step reports an error of 1.0 (generic and specialised
+    kernels)."""
+    with cl.LLContext(q, n) as c:
+        c.load_digits(np.full(n, 1 << 29, dtype=np.int32), 5)
+        assert c.step(1, report=True) == 1.0

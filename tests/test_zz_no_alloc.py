@@ -69,3 +69,35 @@ def test_static_entry_point_rejects_sizes_beyond_its_maximum():
     d = torch.zeros(8, dtype=torch.int32, device="cuda")
     rc, _ = static_step(q, n, 0, 1, d, d)
     assert rc == native.LL_ERR_ARG
+
+
+@pytest.mark.parametrize("q,n", [(86243, 4096),      # generic kernels
+                                 (216091, 12288),    # specialised wide pass, generic tall pass
+                                 (1257787, 65536)])  # specialised passes
+def test_static_entry_point_reports_words_beyond_fp64_range(q, n):
+    """Digits far outside the balanced range make the squared words exceed
+    2^51, where a double has no fraction bits left for the roundoff reading.
+    The kernels flag it, and the call reports the largest possible error (as
+    ll_step does) so that a caller's roundoff policy rejects the result."""
+    import torch
+    d = torch.full((n,), 1 << 29, dtype=torch.int32, device="cuda")
+    out = torch.zeros(n, dtype=torch.int32, device="cuda")
+    for k in (1, 2):
+        rc, err = static_step(q, n, 5, k, d, out)
+        assert rc == 0
+        assert err == 1.0, (k, err)
+    # a valid state afterwards is unaffected by the shared scratch's contents
+    with cl.LLContext(q, n) as c:
+        c.start(5)
+        d0, o0 = c.read_digits()
+        c.step(40, report=True)
+        want = c.res64()
+    rc, err = static_step(q, n, o0, 40, torch.from_numpy(d0.copy()).cuda(), out)
+    assert rc == 0 and err < 0.4
+    assert cl.digits_res64(out.cpu().numpy(), q, n, c_offset(q, o0, 40)) == want
+
+
+def c_offset(q, off, k):
+    for _ in range(k):
+        off = (2 * off) % q
+    return off
