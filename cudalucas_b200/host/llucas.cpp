@@ -50,13 +50,14 @@ struct Config {
   uint32_t fft_len = 0;     // -f / FFTLength
   bool quiet_ini = false;
   // Fault-injection hook for the recovery tests: LLUCAS_INJECT_FAILURES=J:C
-  // makes the C ll_step calls made once the test reaches iteration J fail
-  // on the host (ll_debug_inject_failure), once per process.
+  // makes C ll_step calls fail on the host (ll_debug_inject_failure): the
+  // first call at or after iteration J fails, and after each restart the
+  // next such call fails again, C times in all per process.
   uint32_t inject_at = 0;
   int inject_count = 0;
 };
 
-static bool g_injected = false;
+static int g_inject_left = -1;  // -1: not yet armed from the Config
 
 static bool shape_for(const Config &cfg, uint32_t n, ll_tuning &tu);
 
@@ -254,8 +255,11 @@ static bool read_ck_file(const std::string &name, uint32_t q, Checkpoint &ck, bo
   ck.words.assign(ck.end + 10, 0);
   size_t got = fread(ck.words.data(), 4, ck.words.size(), f);
   fclose(f);
+  // messages of read_checkpoint, CUDALucas.cu:1765-1792
+  const char *bad = backup ? "\nThe backup appears to be corrupt. Restarting test.\n"
+                           : "\nThe checkpoint appears to be corrupt. Trying the backup file.\n";
   if (got != ck.words.size()) {
-    fprintf(stderr, "\nThe %s appears to be corrupt.\n", backup ? "backup" : "checkpoint");
+    fputs(bad, stderr);
     return false;
   }
   const uint32_t stored = ck.words[ck.end + 9];
@@ -265,7 +269,7 @@ static bool read_ck_file(const std::string &name, uint32_t q, Checkpoint &ck, bo
   // validate there; here either checksum is accepted for the backup.
   bool ok = stored == crc || (backup && stored == ll_additive_checksum(ck.words.data(), ck.end + 9));
   if (!ok || ck.words[ck.end] != q) {
-    fprintf(stderr, "\nThe %s appears to be corrupt.\n", backup ? "backup" : "checkpoint");
+    fputs(bad, stderr);
     return false;
   }
   ck.valid = true;
@@ -397,11 +401,13 @@ static int round_off_test(ll_ctx *c, uint32_t q, uint32_t n, uint32_t &j, uint32
   return 0;
 }
 
-// Applies the LLUCAS_INJECT_FAILURES hook once the test has reached it.
+// Applies the LLUCAS_INJECT_FAILURES hook: one failing ll_step call each
+// time the test reaches iteration J, until C calls have failed.
 static void maybe_inject(const Config &cfg, ll_ctx *c, uint32_t j) {
-  if (!g_injected && cfg.inject_count > 0 && j >= cfg.inject_at) {
-    ll_debug_inject_failure(c, cfg.inject_count);
-    g_injected = true;
+  if (g_inject_left < 0) g_inject_left = cfg.inject_count;
+  if (g_inject_left > 0 && j >= cfg.inject_at) {
+    ll_debug_inject_failure(c, 1);
+    --g_inject_left;
   }
 }
 

@@ -114,3 +114,145 @@ def test_cli_selftest(cli, tmp_path):
     r = run(cli, "-r", "0", cwd=str(tmp_path))
     assert r.returncode == 0, r.stdout[-2000:]
     assert r.stdout.count("This residue is correct.") == 20
+
+
+# ------------------------------------------------- recovery and round-off --
+def run_until(cmd, cwd, pattern, timeout=300, env=None):
+    """Runs cmd, sends SIGINT once a stdout line contains `pattern`, and
+    returns (returncode, stdout, stderr)."""
+    import signal
+    import threading
+    p = subprocess.Popen(cmd, cwd=str(cwd), stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                         env=env)
+    out, err = [], []
+    t = threading.Thread(target=lambda: err.extend(p.stderr), daemon=True)
+    t.start()
+    sent = False
+    for line in p.stdout:
+        out.append(line)
+        if not sent and pattern in line:
+            p.send_signal(signal.SIGINT)
+            sent = True
+    rc = p.wait(timeout=timeout)
+    t.join(timeout=10)
+    return rc, "".join(out), "".join(err)
+
+
+def final_line(tmp_path):
+    return (tmp_path / "results.txt").read_text().strip().split("\n")[-1]
+
+
+@pytest.mark.gpu
+def test_cli_roundoff_test_before_a_fresh_test(cli, tmp_path):
+    """RoundoffTest=1: 1000 careful iterations with the error read after
+    each one (CUDALucas.cu:2589-2648), then the test continues."""
+    (tmp_path / "CUDALucas.ini").write_text(INI + "RoundoffTest=1\n")
+    r = run(cli, "86243", cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    assert "Running careful round off test for 1000 iterations." in r.stdout
+    assert "<= 0.25 (max error = " in r.stdout and "continuing test." in r.stdout
+    assert final_line(tmp_path).startswith("M( 86243 )P, offset = ")
+
+
+@pytest.mark.gpu
+def test_cli_injected_step_failure_restarts_from_last_report(cli, tmp_path):
+    """A failed ll_step (injected on the host, no device fault) is handled as
+    the reference handles a CUDA error in the LL loop (CUDALucas.cu:2938-2950):
+    restart from the last good state; the result is unchanged."""
+    (tmp_path / "CUDALucas.ini").write_text(INI)
+    env = dict(os.environ, LLUCAS_INJECT_FAILURES="55000:2")
+    r = subprocess.run([cli, "216091"], cwd=str(tmp_path), capture_output=True, text=True, timeout=300, env=env)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.count("Resetting device and restarting from last checkpoint.") == 2
+    assert "injected failure" in r.stderr
+    assert "Continuing M216091 @ iteration 50001" in r.stdout
+    assert final_line(tmp_path).startswith("M( 216091 )P, offset = ")
+
+
+@pytest.mark.gpu
+def test_cli_roundoff_policy_retry_longer_fft_and_reset(cli, tmp_path):
+    """ErrorLimit 1 (0.00875 at ErrorIterations 100): the 4K length's real
+    roundoff for M86243 (21 bits per word) exceeds it, the 8K length's does
+    not.  The policy of CUDALucas.cu:3043-3097 retries from the last
+    checkpoint, moves to the next length until the next checkpoint, goes
+    back ("Resettng fft.") and repeats; the test still completes."""
+    (tmp_path / "CUDALucas.ini").write_text(INI.replace("ErrorLimit=40", "ErrorLimit=1"))
+    r = run(cli, "-f", "4K", "86243", cwd=str(tmp_path))
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr
+    out = r.stdout
+    assert "Round off error at iteration = " in out
+    assert "Restarting from last checkpoint to see if the error is repeatable." in out
+    assert "The error persists.\nTrying a larger fft until the next checkpoint." in out
+    assert "Resettng fft." in out
+    assert final_line(tmp_path).startswith("M( 86243 )P, offset = ")
+
+
+@pytest.mark.gpu
+def test_cli_roundoff_policy_gives_up(cli, tmp_path):
+    """ErrorLimit 0: every length exceeds it, so after the retry and the
+    longer length the policy gives up (CUDALucas.cu:3060-3064)."""
+    (tmp_path / "CUDALucas.ini").write_text(INI.replace("ErrorLimit=40", "ErrorLimit=0"))
+    r = run(cli, "-f", "4K", "86243", cwd=str(tmp_path))
+    assert r.returncode == 2
+    assert "The error won't go away. I give up." in r.stdout
+    assert not (tmp_path / "results.txt").exists()
+
+
+@pytest.mark.gpu
+def test_cli_resume_at_another_length_and_from_the_backup(cli, tmp_path):
+    """Checkpoints written at 12K resume at 14K (the packed residue does not
+    depend on the length, CUDALucas.cu:1366-1372); a corrupt c<q> falls back
+    to t<q>, the previous checkpoint (CUDALucas.cu:1765-1792)."""
+    (tmp_path / "CUDALucas.ini").write_text(INI)
+    q = 216091
+    rc, out, err = run_until([cli, "-f", "12K", str(q)], tmp_path, "Iteration 30000 ")
+    assert rc in (0, 1), err
+    assert (tmp_path / ("c%d" % q)).exists() and (tmp_path / ("t%d" % q)).exists()
+    raw = bytearray((tmp_path / ("c%d" % q)).read_bytes())
+    raw[100] ^= 0xFF
+    (tmp_path / ("c%d" % q)).write_bytes(bytes(raw))
+    r = run(cli, "-f", "14K", str(q), cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    assert "The checkpoint appears to be corrupt. Trying the backup file." in r.stderr
+    assert "with fft length 14K" in r.stdout
+    assert final_line(tmp_path).startswith("M( %d )P, offset = " % q)
+
+
+REF = os.path.join(ROOT, "oracle", "_ref", "CUDALucas")
+REF_INI = ("WorkFile=worktodo.txt\nResultsFile=results.txt\nSaveAllCheckpoints=0\nSaveFolder=savefiles\n"
+           "DeviceNumber=0\nPrintDeviceInfo=0\nErrorIterations=100\nReportIterations=10000\n"
+           "CheckpointIterations=10000\nPolite=0\nPoliteValue=50\nBigCarry=0\nErrorReset=85\nInteractive=0\n"
+           "RoundoffTest=0\nThreads=256 128\nOutputHInterval=0\nSleep=0\nSleepValue=0\nErrorLimit=40\n")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference binary not built (make -C oracle ref)")
+def test_checkpoint_written_by_the_reference_resumes_in_llucas(cli, tmp_path):
+    """CUDALucas itself writes c216091 (interrupted with SIGINT, which makes
+    it write a checkpoint and exit); llucas continues from that file to the
+    prime verdict."""
+    (tmp_path / "CUDALucas.ini").write_text(REF_INI)
+    q = 216091
+    rc, out, err = run_until([REF, "-f", "12K", str(q)], tmp_path, "Iteration 40000 ")
+    assert (tmp_path / ("c%d" % q)).exists(), out[-2000:] + err
+    raw = (tmp_path / ("c%d" % q)).read_bytes()
+    assert len(raw) == 4 * ((q + 31) // 32 + 10)
+    r = run(cli, str(q), cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    assert "Continuing M%d @ iteration " % q in r.stdout
+    assert final_line(tmp_path).startswith("M( %d )P, offset = " % q)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference binary not built (make -C oracle ref)")
+def test_checkpoint_written_by_llucas_resumes_in_the_reference(cli, tmp_path):
+    """llucas writes c216091; CUDALucas itself continues from that file to the
+    prime verdict (the byte layout and CRC are the reference's)."""
+    (tmp_path / "CUDALucas.ini").write_text(REF_INI)
+    q = 216091
+    rc, out, err = run_until([cli, "-f", "12K", str(q)], tmp_path, "Iteration 40000 ")
+    assert rc in (0, 1), err
+    assert (tmp_path / ("c%d" % q)).exists()
+    r = subprocess.run([REF, str(q)], cwd=str(tmp_path), capture_output=True, text=True, timeout=300)
+    assert "Continuing M%d @ iteration " % q in r.stdout, r.stdout[-2000:]
+    assert "M( %d )P" % q in r.stdout, r.stdout[-2000:]
