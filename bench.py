@@ -400,17 +400,22 @@ def run_reference(args, world, rank, local):
 def run_batch(args, world, rank, local):
     """Batched mode: 256 primes log-uniform in [1e6, 2e7] (seed 7) at the
     length policy's FFT lengths, all advancing together (one CUDA graph per
-    step), against the same exponents run one at a time."""
+    step), against the same exponents run one at a time over the same
+    iterations.  The first step of the batch (S iterations, reported) is
+    compared member by member with the solo runs."""
     import torch
     import cudalucas_b200 as cl
     from cudalucas_b200 import workloads
     torch.cuda.set_device(local)
     members = workloads.batch_exponents(args.batch_count, seed=7 + rank)
     qs, ns = zip(*members)
+    offs = [(q * 7) // 11 for q in qs]
     S, K, W = args.iters_per_step, args.steps, args.warmup
     b = cl.LLBatch(qs, ns, device=local, graph_iters=args.batch_graph_iters)
-    b.start([(q * 7) // 11 for q in qs])
-    for _ in range(W):
+    b.start(offs)
+    b.step(S, report=True)           # the first warm-up step, checked against solo runs below
+    res_batch = b.res64()
+    for _ in range(W - 1):
         b.step(S)
     b.sync()
     ext = torch.cuda.ExternalStream(b.stream, device=torch.device("cuda", local))
@@ -425,22 +430,24 @@ def run_batch(args, world, rank, local):
         b.sync()
     ms = allreduce_max(t0.elapsed_time(t1), world)
     errs = b.step(1, report=True)
-    res = b.res64()
     b.close()
-    # the same exponents one at a time (bounded sample of iterations each)
-    Ss = args.serial_iters
+    # the same exponents one at a time, each the same S iterations from the
+    # same offset: the serial baseline, and Res64 equal to the batch's
+    Ss = args.serial_iters or S
     serial_ms = 0.0
-    for q, n in members:
+    mismatched = []
+    for (q, n), off, rb in zip(members, offs, res_batch):
         c = cl.LLContext(q, n, device=local)
-        c.start(1)
-        c.step(20)
+        c.start(off)
         ext1 = torch.cuda.ExternalStream(c.stream, device=torch.device("cuda", local))
         a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a0.record(ext1)
-        c.step(Ss)
+        c.step(Ss, report=True, wait=False)
         a1.record(ext1)
         c.sync()
         serial_ms += a0.elapsed_time(a1)
+        if Ss == S and c.res64() != rb:
+            mismatched.append(q)
         c.close()
     serial_ms = allreduce_max(serial_ms, world)
     if rank != 0:
@@ -456,9 +463,11 @@ def run_batch(args, world, rank, local):
                                % (len(members), min(ns) // 1024, max(ns) // 1024),
                    "iters_per_step": S, "graph_iters": args.batch_graph_iters,
                    "serial_iter_s": round(serial_ips, 1), "speedup_vs_serial": round(batch_ips / serial_ips, 3),
-                   "serial_sample": "%d iterations of each exponent alone" % Ss,
-                   "max_roundoff_error": round(float(max(errs)), 5),
-                   "res64_xor": "%016x" % (__import__("functools").reduce(lambda a, b: a ^ b, res))},
+                   "serial_sample": "%d iterations of each exponent alone, from the batch's offsets" % Ss,
+                   "max_roundoff_error": round(float(max(errs)), 5)},
+        "res64_ok": Ss == S and not mismatched,
+        "res64_checked": {"against": "each member run alone for the same %d iterations" % S,
+                          "members": len(members) if Ss == S else 0, "mismatched": mismatched},
         "clocks": clk.summary(),
         "gpu_launches": 2 * len(members) * K * S,
     }
@@ -481,10 +490,11 @@ def run_serve(args, world, rank, local):
         r.iters = 50
     serve.Server(eng).run(warm, realtime=False)
     barrier(world)
+    srv = serve.Server(eng, chunk=args.serve_chunk, hbm_cap=args.serve_hbm_gb * 1e9)
     with Clocks(local) as clk:
-        batched = serve.Server(eng, chunk=args.serve_chunk).run(mk())
+        batched = srv.run(mk())
     serial = serve.serve_serial(eng, mk())
-    same = all(a.res64 == b.res64 for a, b in zip(batched, serial))
+    same = all(a.res64 == b.res64 and a.error is None for a, b in zip(batched, serial))
     sb, ss = serve.summary(batched), serve.summary(serial)
     if rank != 0:
         return None
@@ -495,10 +505,13 @@ def run_serve(args, world, rank, local):
         "data": "synthetic: seeded Poisson arrivals of LL requests",
         "config": {"workload": "serve: %d requests, Poisson 50/s, p log-uniform [1e5, 5e7], k uniform [1e3, 5e4], "
                                "seed 11" % len(reqs), "chunk_iters": args.serve_chunk,
+                   "hbm_cap_bytes": srv.hbm_cap, "peak_device_bytes": srv.peak_bytes,
+                   "peak_active_requests": srv.peak_active,
                    "continuous": sb, "serial": ss, "results_identical": same,
                    "speedup_p50": round(ss["p50_s"] / sb["p50_s"], 3),
                    "speedup_throughput": round(sb["iter_per_s"] / ss["iter_per_s"], 3)},
         "p99": round(sb["p99_s"], 4),
+        "res64_ok": same,
         "clocks": clk.summary(),
     }
 
@@ -515,7 +528,9 @@ def main():
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--batch-graph-iters", type=int, default=10,
                     help="iterations of every member per CUDA graph in the batch workload")
-    ap.add_argument("--serial-iters", type=int, default=200)
+    ap.add_argument("--serial-iters", type=int, default=0,
+                    help="iterations of each exponent alone in the batch workload's serial leg (0: the step size)")
+    ap.add_argument("--serve-hbm-gb", type=float, default=150.0)
     ap.add_argument("--iters-per-step", type=int, default=10000)
     ap.add_argument("--cpu-iters", type=int, default=20,
                     help="oracle iterations on one host thread for cpu_baseline (0: skip)")

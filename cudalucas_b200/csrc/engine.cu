@@ -35,6 +35,7 @@
 // touch the state.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -643,6 +644,9 @@ struct ll_ctx {
   // device buffers
   double2 *A = nullptr;
   int32_t *xint = nullptr;
+  int32_t *ck_digits = nullptr;  // device-resident checkpoint (allocated on first use)
+  uint32_t ck_offset = 0;
+  bool ck_valid = false;
   long long *carry = nullptr;
   uint32_t *flags = nullptr;
   DevState *st = nullptr;
@@ -691,7 +695,7 @@ static void free_ctx(ll_ctx *c) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
-  void *ptrs[] = {c->A, c->xint, c->carry, c->flags, c->st, c->twW, c->twH, c->thi, c->tlo, c->stwW, c->stwH,
+  void *ptrs[] = {c->A, c->xint, c->ck_digits, c->carry, c->flags, c->st, c->twW, c->twH, c->thi, c->tlo, c->stwW, c->stwH,
                   c->rowE, c->colF, c->rowW, c->rowWi, c->colW, c->colWi};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1039,6 +1043,55 @@ ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
     }
   }
   return LL_OK;
+}
+
+ll_status ll_device_checkpoint(ll_ctx *ctx) {
+  if (!ctx) return LL_ERR_ARG;
+  if (!ctx->digits_current) return LL_ERR_STATE;
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->ck_digits) {
+    const cudaError_t e = cudaMalloc((void **)&ctx->ck_digits, sizeof(int32_t) * ctx->n);
+    if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? LL_ERR_NOMEM : cuda_fail(ctx, e, "cudaMalloc");
+  }
+  CK(cudaMemcpyAsync(ctx->ck_digits, ctx->xint, sizeof(int32_t) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+  ctx->ck_offset = ctx->offset;
+  ctx->ck_valid = true;
+  return LL_OK;
+}
+
+ll_status ll_device_restore(ll_ctx *ctx, uint32_t *offset) {
+  if (!ctx) return LL_ERR_ARG;
+  if (!ctx->ck_valid) return LL_ERR_STATE;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(ctx->xint, ctx->ck_digits, sizeof(int32_t) * ctx->n, cudaMemcpyDeviceToDevice, ctx->stream));
+  // offset, roundoff maximum and fault bits; the ticket counter is kept
+  const uint32_t f[3] = {ctx->ck_offset, 0u, 0u};
+  static_assert(offsetof(DevState, err_bits) == offsetof(DevState, offset) + 4 &&
+                    offsetof(DevState, fault) == offsetof(DevState, offset) + 8,
+                "offset, err_bits and fault are contiguous");
+  CK(cudaMemcpyAsync(&ctx->st->offset, f, sizeof f, cudaMemcpyHostToDevice, ctx->stream));
+  const ll_status rc = launch_init(ctx);
+  if (rc != LL_OK) return rc;
+  ctx->offset = ctx->ck_offset;
+  ctx->digits_current = true;
+  ctx->started = true;
+  if (offset) *offset = ctx->offset;
+  return LL_OK;
+}
+
+uint64_t ll_context_bytes(uint32_t q, uint32_t n, const ll_tuning *tuning) {
+  Shape s;
+  if (n < 64 || n % 4 || !choose_shape((long long)n / 2, tuning, s)) return 0;
+  (void)q;
+  const uint64_t N = n / 2, W = (uint64_t)s.W, H = (uint64_t)s.H, ng = (uint64_t)(s.H / s.G);
+  int ts = 0;
+  while ((1 << (ts + 1)) * (long long)(1 << (ts + 1)) <= (long long)N * 4 && ts < 14) ++ts;
+  uint64_t b = 16 * N + 4ull * n + 8 * ng * W + 4 * kWarpFlags * ng + sizeof(DevState);  // state, digits, carries
+  b += 16 * (W + H) + 16 * (((uint64_t)1 << ts) + (N >> ts) + 1);                     // twiddles
+  b += 20 * 2 * H + 20 * W;                                                           // weights
+  if (s.sw) b += 16 * (uint64_t)s.sw->extra;
+  if (s.st) b += 16 * (uint64_t)s.st->tw;
+  return b;
 }
 
 int32_t ll_busy(ll_ctx *ctx) {

@@ -99,6 +99,16 @@ class LLContext:
             raise LLError(native.LL_ERR_CUDA, "ll_busy")
         return bool(r)
 
+    def device_checkpoint(self):
+        """Keeps a device copy of the digits of the last report step."""
+        self._check(native.lib().ll_device_checkpoint(self._h), "ll_device_checkpoint")
+
+    def device_restore(self):
+        """Reloads the state from the device checkpoint; returns its offset."""
+        off = ctypes.c_uint32(0)
+        self._check(native.lib().ll_device_restore(self._h, ctypes.byref(off)), "ll_device_restore")
+        return int(off.value)
+
     def debug_launch(self, which):
         self._check(native.lib().ll_debug_launch(self._h, int(which)), "ll_debug_launch")
 
@@ -267,6 +277,11 @@ def fft_prune(lengths, ms_per_iter):
 
 def fft_max_exponent(n):
     return int(native.lib().ll_fft_max_exponent(int(n)))
+
+
+def context_bytes(q, n):
+    """Device memory of a context for (q, n) in bytes (0: unsupported length)."""
+    return int(native.lib().ll_context_bytes(int(q), int(n), None))
 
 
 def device_name(device=0):

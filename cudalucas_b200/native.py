@@ -53,6 +53,9 @@ def lib():
         "ll_res64": (i32, [vp, ctypes.POINTER(u64)]),
         "ll_sync": (i32, [vp]),
         "ll_busy": (i32, [vp]),
+        "ll_device_checkpoint": (i32, [vp]),
+        "ll_device_restore": (i32, [vp, u32p]),
+        "ll_context_bytes": (u64, [u32, u32, ctypes.POINTER(Tuning)]),
         "ll_exponent": (u32, [vp]),
         "ll_fft_length": (u32, [vp]),
         "ll_offset": (u32, [vp]),

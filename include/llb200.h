@@ -89,6 +89,22 @@ ll_status ll_read_digits(ll_ctx *ctx, int32_t *digits, uint32_t *offset);
  * current digits like ll_read_digits. */
 ll_status ll_res64(ll_ctx *ctx, uint64_t *res64);
 
+/* Device-resident checkpoint (no counterpart in the reference, which keeps
+ * its restart point packed on the host, CUDALucas.cu:2963-2980).
+ * ll_device_checkpoint enqueues a device-to-device copy of the digits the
+ * last LL_REPORT step wrote (LL_ASYNC included) into a buffer the context
+ * owns (4n bytes, allocated by the first call) and remembers their offset.
+ * ll_device_restore enqueues the reload of the state from that copy (as
+ * ll_load_digits does from the host) and returns the restored offset;
+ * neither call waits for the GPU. */
+ll_status ll_device_checkpoint(ll_ctx *ctx);
+ll_status ll_device_restore(ll_ctx *ctx, uint32_t *offset);
+
+/* Device memory a context for (q, n) allocates, in bytes (its state array,
+ * digits, carry rows, flags and tables; the device checkpoint adds 4n), or
+ * 0 if the length is not supported.  Host-only. */
+uint64_t ll_context_bytes(uint32_t q, uint32_t n, const ll_tuning *tuning);
+
 /* Waits for all queued work of the context. */
 ll_status ll_sync(ll_ctx *ctx);
 
