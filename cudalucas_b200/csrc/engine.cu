@@ -384,17 +384,23 @@ struct StaticTall {
   int L;
   void (*run)(TallArgs);
   int nrad, rad[4];
-  int extra;  // shared-memory entries beyond the two columns
-  int tw;     // of which stage twiddles (the first entries)
+  int tw;       // stage twiddle entries
+  int smem;     // shared-memory entries of a CTA
+  int threads;  // threads per CTA
+  int ppc;      // column pairs per CTA
 };
 
 #define LLB_WIDE(LIST, G)                                                                                       \
   {LIST::L, G, wide_static<LIST, G, WIDE_ITER>, wide_static<LIST, G, WIDE_REPORT>, wide_static<LIST, G, WIDE_INIT>, \
    LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tw_size<LIST>(),             \
    G * row_slots<LIST::L, G>()}
+#define LLB_RAD(LIST) LIST::N, {LIST::a[0], LIST::N > 1 ? LIST::a[1 % LIST::N] : 0, LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}
 #define LLB_TALL(LIST) \
-  {LIST::L, tall_static<LIST>, LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, \
-   tall_extra<LIST>(), tw_size<LIST>()}
+  {LIST::L, tall_static<LIST>, LLB_RAD(LIST), tw_size<LIST>(), padded(2 * LIST::L) + tall_extra<LIST>(), 2 * (LIST::L / 16), 1}
+// any radix list: TC threads per column, PP column pairs per CTA
+#define LLB_TALL_ANY(LIST, TC, PP)                                                                       \
+  {LIST::L, tall_any<LIST, TC, PP>, LLB_RAD(LIST), tw_size<LIST>(), 2 * PP * col_slots<LIST::L>() + tw_size<LIST>(), \
+   2 * PP * TC, PP}
 
 using L256 = RList<16, 16>;
 using L512 = RList<16, 2, 16>;
@@ -409,15 +415,62 @@ using L2560 = RList<16, 10, 16>;
 using L3072 = RList<16, 12, 16>;
 using L3584 = RList<16, 14, 16>;
 using L4096 = RList<16, 16, 16>;
+// column lengths of the tall_any kernels
+using C24 = RList<12, 2>;
+using C28 = RList<14, 2>;
+using C100 = RList<10, 10>;
+using C112 = RList<16, 7>;
+using C120 = RList<12, 10>;
+using C140 = RList<14, 10>;
+using C160 = RList<16, 10>;
+using C168 = RList<14, 12>;
+using C192 = RList<16, 12>;
+using C224 = RList<16, 14>;
+using C240 = RList<12, 10, 2>;
+using C252 = RList<14, 9, 2>;
+using C288 = RList<16, 9, 2>;
+using C320 = RList<16, 10, 2>;
+using C336 = RList<14, 12, 2>;
+using C360 = RList<10, 9, 4>;
+using C392 = RList<14, 14, 2>;
+using C400 = RList<10, 10, 4>;
+using C448 = RList<16, 14, 2>;
+using C576 = RList<12, 12, 4>;
+using C600 = RList<12, 10, 5>;
+using C648 = RList<12, 9, 6>;
+using C672 = RList<14, 12, 4>;
+using C720 = RList<12, 10, 6>;
+using C784 = RList<16, 7, 7>;
+using C800 = RList<16, 10, 5>;
+using C1568 = RList<16, 14, 7>;
+using C2744 = RList<14, 14, 14>;
 
 static const StaticWide kWide[] = {
     LLB_WIDE(L256, 4),  LLB_WIDE(L512, 4),  LLB_WIDE(L768, 4),  LLB_WIDE(L1024, 2), LLB_WIDE(L1280, 2),
     LLB_WIDE(L1536, 2), LLB_WIDE(L1792, 2), LLB_WIDE(L2048, 2), LLB_WIDE(L2304, 2),
     LLB_WIDE(L2560, 2), LLB_WIDE(L3072, 2), LLB_WIDE(L3584, 1), LLB_WIDE(L4096, 1),
 };
+// Column lengths outside the 16 x M x 16 family that the length policy meets
+// with a specialised row length: the fewest stages of radices <= 16, and the
+// fewest threads per column that keep a stage's butterflies of one thread
+// within 16 elements; about 256 threads per CTA.
 static const StaticTall kTall[] = {
     LLB_TALL(L256),  LLB_TALL(L512),  LLB_TALL(L768),  LLB_TALL(L1024), LLB_TALL(L1280), LLB_TALL(L1536), LLB_TALL(L1792),
     LLB_TALL(L2048), LLB_TALL(L2304), LLB_TALL(L2560), LLB_TALL(L3072), LLB_TALL(L3584), LLB_TALL(L4096),
+    LLB_TALL_ANY(C24, 2, 64),        LLB_TALL_ANY(C28, 2, 64),
+    LLB_TALL_ANY(C100, 10, 12),      LLB_TALL_ANY(C112, 8, 16),
+    LLB_TALL_ANY(C120, 12, 10),      LLB_TALL_ANY(C140, 14, 9),
+    LLB_TALL_ANY(C160, 16, 8),       LLB_TALL_ANY(C168, 14, 9),
+    LLB_TALL_ANY(C192, 16, 8),       LLB_TALL_ANY(C224, 16, 8),
+    LLB_TALL_ANY(C240, 24, 5),    LLB_TALL_ANY(C252, 28, 4),
+    LLB_TALL_ANY(C288, 32, 4),     LLB_TALL_ANY(C320, 32, 4),
+    LLB_TALL_ANY(C336, 28, 4),    LLB_TALL_ANY(C360, 40, 3),
+    LLB_TALL_ANY(C392, 28, 4),    LLB_TALL_ANY(C400, 40, 3),
+    LLB_TALL_ANY(C448, 32, 4),    LLB_TALL_ANY(C576, 48, 2),
+    LLB_TALL_ANY(C600, 60, 2),    LLB_TALL_ANY(C648, 72, 1),
+    LLB_TALL_ANY(C672, 56, 2),    LLB_TALL_ANY(C720, 72, 1),
+    LLB_TALL_ANY(C784, 56, 2),     LLB_TALL_ANY(C800, 80, 1),
+    LLB_TALL_ANY(C1568, 112, 1),   LLB_TALL_ANY(C2744, 196, 1),
 };
 
 static const StaticWide *find_wide(int L) {
@@ -548,7 +601,7 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
       out.H = (int)(N / bw->L);
       out.G = bw->G;
       out.T1 = bw->G * (bw->L / 16);
-      out.T2 = 2 * (out.H / 16);
+      out.T2 = bt->threads;
       out.sw = bw;
       out.st = bt;
       return true;
@@ -610,8 +663,10 @@ size_t shape_wide_smem(const Shape &s) {
   return wide_smem(s.W, s.G);
 }
 size_t shape_tall_smem(const Shape &s) {
-  return tall_smem(s.H) + (s.st ? sizeof(double2) * (size_t)s.st->extra : 0);
+  return s.st ? sizeof(double2) * (size_t)s.st->smem : tall_smem(s.H);
 }
+// CTAs of the tall pass
+int tall_grid(const Shape &s) { return s.st ? (s.W / 2 + s.st->ppc - 1) / s.st->ppc : s.W / 2; }
 
 // Stage twiddles of a radix list in the order the specialised kernels read
 // them: for each stage with NS > 1, rows k < NS of w_{NS*R}^(r*k), r = 1..R-1,
@@ -859,7 +914,7 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
           cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, s.st->run, s.T2, shape_tall_smem(s)) == cudaSuccess &&
           bw > 0 && bt > 0) {
         const long long ww = ((long long)(s.H / s.G) + (long long)sms * bw - 1) / ((long long)sms * bw);
-        const long long wt = ((long long)(s.W / 2) + (long long)sms * bt - 1) / ((long long)sms * bt);
+        const long long wt = ((long long)tall_grid(s) + (long long)sms * bt - 1) / ((long long)sms * bt);
         ctx->pdl = ww <= 4 && wt <= 4;
       }
     }
@@ -933,7 +988,7 @@ static void launch_wide(ll_ctx *ctx, int mode, bool chained = false) {
 
 static void launch_tall(ll_ctx *ctx, bool chained = false) {
   const Shape &s = ctx->shape;
-  if (s.st) launch_static((const void *)s.st->run, &ctx->ta, s.W / 2, s.T2, shape_tall_smem(s), ctx->stream, chained && ctx->pdl);
+  if (s.st) launch_static((const void *)s.st->run, &ctx->ta, tall_grid(s), s.T2, shape_tall_smem(s), ctx->stream, chained && ctx->pdl);
   else tall_kernel<EPT><<<s.W / 2, s.T2, tall_smem(s.H), ctx->stream>>>(ctx->ta);
 }
 
@@ -1145,6 +1200,10 @@ void ll_shape(const ll_ctx *ctx, int32_t *width, int32_t *height, int32_t *rows_
   if (threads_tall) *threads_tall = ctx->shape.T2;
 }
 const char *ll_last_error(const ll_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+int32_t ll_kernel_kinds(const ll_ctx *ctx) {
+  if (!ctx) return 0;
+  return (ctx->shape.sw ? 1 : 0) | (ctx->shape.st ? 2 : 0);
+}
 void ll_debug_inject_failure(ll_ctx *ctx, int32_t count) {
   if (ctx) ctx->inject = count;
 }
@@ -1391,7 +1450,7 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
   table_lock.unlock();  // the pageable-source copies above have consumed the host tables
 
   // ---- digits in -> weighted transform -> iters iterations -> digits out
-  const dim3 gw(H / s.G), gt(W / 2);
+  const dim3 gw(H / s.G), gt(tall_grid(s));
   wa.xint = const_cast<int32_t *>(digits_in);
   if (s.sw) s.sw->init<<<gw, s.T1, sw_bytes, st>>>(wa);
   else wide_kernel<EPT, WIDE_INIT><<<gw, s.T1, sw_bytes, st>>>(wa);

@@ -406,6 +406,89 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
   for (int r = 0; r < 16; ++r) dst[t + r * TR] = cmulc(o[r], cmul(base, wr[col * 16 + r]));
 }
 
+// All stages of the radix list P in list order, in shared memory (Stockham:
+// natural order in and out); SIGN -1 with conjugate twiddles is the inverse
+// transform over the same twiddle table.
+template <class P, int RS, int I, int NS, int TR, int SIGN>
+__device__ __forceinline__ void all_stages(double2 *s, const double2 *tw, int row, int t) {
+  if constexpr (I < P::N) {
+    constexpr int R = P::a[I];
+    sstage<P::L, RS, R, NS, SIGN, TR>(s, tw + tw_offset<P, I>(), row, t);
+    all_stages<P, RS, I + 1, NS * R, TR, SIGN>(s, tw, row, t);
+  }
+}
+
+// Tall pass for column lengths H = P::L outside the 16 x M x 16 family (any
+// radix list of 2..16): PP column pairs per CTA, TC threads per column, every
+// stage in shared memory.  A column is loaded with the twiddle w_N^(k1*m2)
+// applied, transformed, paired by index with its mirror column (bins k2 and
+// H-1-k2; pair 0 holds the self-paired columns 0 and W/2), transformed back
+// with conjugate twiddles and stored with the conjugate twiddle.  The same
+// arithmetic as the generic tall kernel, with every index and loop bound a
+// constant.
+template <class P, int TC, int PP>
+__global__ void __launch_bounds__(2 * PP * TC, min_blocks(2 * PP * TC)) tall_any(TallArgs a) {
+  constexpr int H = P::L, CS = col_slots<H>(), T = 2 * PP * TC;
+  extern __shared__ double2 sm[];
+  double2 *stw = sm + 2 * PP * CS;
+  const int units = a.W / 2;
+  const int col = threadIdx.x / TC, t = threadIdx.x - col * TC;  // col < 2*PP
+  const int pl = col >> 1;
+  const int c = blockIdx.x * PP + pl;  // column pair
+  const bool active = c < units;
+  const bool special = c == 0;
+  const int W = a.W;
+  const int kA = special ? 0 : c, kB = special ? W / 2 : W - c;
+  const int k1 = (col & 1) ? kB : kA;
+  for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
+  griddep_wait();
+  griddep_release();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const uint32_t o = a.st->offset;  // CUDALucas.cu:1882, once per iteration
+    a.st->offset = (uint32_t)((2ull * o) % a.q);
+  }
+  double2 *row = sm + col * CS;
+  if (active) {
+    const double2 *src = a.A + (size_t)k1 * H;
+    for (int m2 = t; m2 < H; m2 += TC) row[pad(m2)] = cmul(src[m2], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  all_stages<P, CS, 0, 1, TC, +1>(sm, stw, col, t);
+  if (active) {
+    const int ti = threadIdx.x - 2 * pl * TC;  // thread of the pair, < 2*TC
+    double2 *ra = sm + 2 * pl * CS, *rb = ra + CS;
+    if (!special) {
+      for (int k2 = ti; k2 < H; k2 += 2 * TC) {  // bin k2 of column kA <-> bin H-1-k2 of column kB
+        double2 za = ra[pad(k2)], zb = rb[pad(H - 1 - k2)];
+        pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, kA + W * k2));
+        ra[pad(k2)] = za;
+        rb[pad(H - 1 - k2)] = zb;
+      }
+    } else {
+      for (int i = ti; i <= H / 2; i += 2 * TC) {  // column 0: k2 <-> (H-k2) mod H
+        const int p2 = (H - i) % H;
+        double2 za = ra[pad(i)], zb = ra[pad(p2)];
+        pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W * i));
+        ra[pad(i)] = za;
+        if (p2 != i) ra[pad(p2)] = zb;
+      }
+      for (int i = ti; i < H / 2; i += 2 * TC) {  // column W/2: k2 <-> H-1-k2
+        double2 za = rb[pad(i)], zb = rb[pad(H - 1 - i)];
+        pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W / 2 + W * i));
+        rb[pad(i)] = za;
+        rb[pad(H - 1 - i)] = zb;
+      }
+    }
+  }
+  __syncthreads();
+  all_stages<P, CS, 0, 1, TC, -1>(sm, stw, col, t);
+  if (active) {
+    double2 *dst = a.A + (size_t)k1 * H;
+    for (int m2 = t; m2 < H; m2 += TC) dst[m2] = cmulc(row[pad(m2)], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
+  }
+}
+
 template <class P, int G>
 constexpr int wide_threads() { return G * (P::L / 16); }
 

@@ -127,7 +127,10 @@ class LLContext:
     def shape(self):
         v = [ctypes.c_int32() for _ in range(5)]
         native.lib().ll_shape(self._h, *[ctypes.byref(x) for x in v])
-        return dict(zip(("W", "H", "G", "threads_wide", "threads_tall"), [x.value for x in v]))
+        d = dict(zip(("W", "H", "G", "threads_wide", "threads_tall"), [x.value for x in v]))
+        k = native.lib().ll_kernel_kinds(self._h)
+        d["wide_specialised"], d["tall_specialised"] = bool(k & 1), bool(k & 2)
+        return d
 
 
 class LLBatch:

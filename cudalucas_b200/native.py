@@ -62,6 +62,7 @@ def lib():
         "ll_stream": (vp, [vp]),
         "ll_shape": (None, [vp, i32p, i32p, i32p, i32p, i32p]),
         "ll_last_error": (ctypes.c_char_p, [vp]),
+        "ll_kernel_kinds": (i32, [vp]),
         "ll_status_string": (ctypes.c_char_p, [i32]),
         "ll_debug_inject_failure": (None, [vp, i32]),
         "ll_debug_launch": (i32, [vp, i32]),

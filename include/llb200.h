@@ -120,6 +120,9 @@ void *ll_stream(const ll_ctx *ctx);           /* the context's cudaStream_t */
 void ll_shape(const ll_ctx *ctx, int32_t *width, int32_t *height,
               int32_t *rows_per_cta, int32_t *threads_wide, int32_t *threads_tall);
 const char *ll_last_error(const ll_ctx *ctx); /* text of the last failure   */
+/* Which passes run compile-time specialised kernels: bit 0 the wide (row)
+ * pass, bit 1 the tall (column) pass; the others use the generic kernels. */
+int32_t ll_kernel_kinds(const ll_ctx *ctx);
 const char *ll_status_string(ll_status s);
 
 /* Test hook (CUDALucas.cu:2938-2950 handles a CUDA error from lucas_square

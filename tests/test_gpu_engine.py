@@ -228,3 +228,36 @@ def test_words_beyond_fp64_range_report_max_error(q, n):
     with cl.LLContext(q, n) as c:
         c.load_digits(np.full(n, 1 << 29, dtype=np.int32), 5)
         assert c.step(1, report=True) == 1.0
+
+
+def _exponent_at(n, bits=17.6):
+    from cudalucas_b200.fftbench import is_prime
+    q = int(n * bits) | 1
+    while not is_prime(q):
+        q += 2
+    return q
+
+
+@pytest.mark.parametrize("nk", [12, 14, 50, 56, 60, 70, 80, 96, 112, 120, 126, 144, 160, 180, 224, 288, 320, 336,
+                                360, 392, 400, 448, 576, 864, 900, 3136])
+def test_specialised_columns_of_any_radix_list(nk):
+    """Lengths whose columns are not 16 x M x 16 (C1's 12K, the batch set's
+    50K-900K, 3136K, the default length of M57885161) run a specialised
+    tall pass (tall_any) and give the oracle's residue."""
+    from oracle.binding import set_threads
+    n = nk * 1024
+    q = _exponent_at(n)
+    k = 12
+    off = q // 5
+    d, o_off, err, shape = engine_run(q, n, off, k)
+    assert shape["tall_specialised"] and shape["wide_specialised"], shape
+    set_threads(8)
+    try:
+        o = Oracle(q, n)
+        o.start(off)
+        oerr = o.step(k)
+        want = o.res64()
+    finally:
+        set_threads(1)
+    assert cl.digits_res64(d, q, n, o_off) == want
+    assert err < 0.4 and err <= 2 * oerr + 1e-3 and oerr <= 2 * err + 1e-3, (err, oerr)
