@@ -376,6 +376,7 @@ struct StaticWide {
   void (*iter)(WideArgs);
   void (*report)(WideArgs);
   void (*init)(WideArgs);
+  void (*iter_batch)(const WideArgs *, int);  // all members of a length class
   int nrad, rad[4];
   int extra;  // shared-memory entries beyond the rows (stage twiddles)
   int rows;   // shared-memory entries of the G rows
@@ -383,6 +384,7 @@ struct StaticWide {
 struct StaticTall {
   int L;
   void (*run)(TallArgs);
+  void (*batch)(const TallArgs *, int);  // all members of a length class
   int nrad, rad[4];
   int tw;       // stage twiddle entries
   int smem;     // shared-memory entries of a CTA
@@ -392,14 +394,17 @@ struct StaticTall {
 
 #define LLB_WIDE(LIST, G)                                                                                       \
   {LIST::L, G, wide_static<LIST, G, WIDE_ITER>, wide_static<LIST, G, WIDE_REPORT>, wide_static<LIST, G, WIDE_INIT>, \
+   wide_static_batch<LIST, G>,                                                                                  \
    LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tw_size<LIST>(),             \
    G * row_slots<LIST::L, G>()}
 #define LLB_RAD(LIST) LIST::N, {LIST::a[0], LIST::N > 1 ? LIST::a[1 % LIST::N] : 0, LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}
 #define LLB_TALL(LIST) \
-  {LIST::L, tall_static<LIST>, LLB_RAD(LIST), tw_size<LIST>(), padded(2 * LIST::L) + tall_extra<LIST>(), 2 * (LIST::L / 16), 1}
+  {LIST::L, tall_static<LIST>, tall_static_batch<LIST>, LLB_RAD(LIST), tw_size<LIST>(),                      \
+   padded(2 * LIST::L) + tall_extra<LIST>(), 2 * (LIST::L / 16), 1}
 // any radix list: TC threads per column, PP column pairs per CTA
 #define LLB_TALL_ANY(LIST, TC, PP)                                                                       \
-  {LIST::L, tall_any<LIST, TC, PP>, LLB_RAD(LIST), tw_size<LIST>(), 2 * PP * col_slots<LIST::L>() + tw_size<LIST>(), \
+  {LIST::L, tall_any<LIST, TC, PP>, tall_any_batch<LIST, TC, PP>, LLB_RAD(LIST), tw_size<LIST>(),          \
+   2 * PP * col_slots<LIST::L>() + tw_size<LIST>(),                                                           \
    2 * PP * TC, PP}
 
 using L256 = RList<16, 16>;
@@ -891,11 +896,13 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
       for (const auto &k : kWide)
         if ((e = cudaFuncSetAttribute(k.iter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
             (e = cudaFuncSetAttribute(k.report, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
-            (e = cudaFuncSetAttribute(k.init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess)
+            (e = cudaFuncSetAttribute(k.init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess ||
+            (e = cudaFuncSetAttribute(k.iter_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw)) != cudaSuccess)
           break;
       for (const auto &k : kTall)
         if (e == cudaSuccess &&
-            (e = cudaFuncSetAttribute(k.run, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess)
+            ((e = cudaFuncSetAttribute(k.run, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess ||
+             (e = cudaFuncSetAttribute(k.batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess))
           break;
       if (e != cudaSuccess) {
         rc = cuda_fail(ctx, e, "cudaFuncSetAttribute (static)");
@@ -1490,12 +1497,30 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
 // the branches fork from and join back to the batch stream, and the GPU runs
 // the independent branches concurrently.  A member runs exactly the kernels it
 // would run alone, so its residues are the solo residues.
+// Members of one FFT length whose passes both have specialised kernels run
+// as a length class: one launch per pass for all of them (blockIdx.x =
+// member * units + unit), the members' kernel arguments in a device array.
+struct BatchClass {
+  std::vector<int> idx;  // members
+  const StaticTall *st = nullptr;
+  const StaticWide *sw = nullptr;
+  TallArgs *d_ta = nullptr;
+  WideArgs *d_wa = nullptr;
+  int tall_units = 0, wide_units = 0, T1 = 0, T2 = 0;
+  size_t smem_t = 0, smem_w = 0;
+  bool pdl = false;
+  cudaStream_t stream = nullptr;
+};
+
 struct ll_batch {
   int device = 0;
   std::vector<ll_ctx *> members;
   cudaStream_t stream = nullptr;
   std::vector<cudaEvent_t> events;  // [0] fork, [1..] joins
   int graph_iters = 0;
+  bool by_class = true;                 // one launch per pass per length class
+  std::vector<BatchClass> classes;
+  std::vector<int> singles;             // members launched on their own
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   std::string err;
@@ -1507,9 +1532,86 @@ static void free_batch(ll_batch *b) {
   if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+  for (BatchClass &k : b->classes) {
+    if (k.d_ta) cudaFree(k.d_ta);
+    if (k.d_wa) cudaFree(k.d_wa);
+    if (k.stream) cudaStreamDestroy(k.stream);
+  }
   if (b->stream) cudaStreamDestroy(b->stream);
   for (ll_ctx *c : b->members) ll_destroy(c);
   delete b;
+}
+
+// Groups the members into length classes (the rest stay singles), uploads
+// the classes' argument arrays and creates a stream per class.
+static ll_status build_classes(ll_batch *b) {
+  std::vector<int> order;
+  for (size_t i = 0; i < b->members.size(); ++i) {
+    const ll_ctx *c = b->members[i];
+    if (!(c->shape.sw && c->shape.st)) {
+      b->singles.push_back((int)i);
+      continue;
+    }
+    BatchClass *k = nullptr;
+    for (BatchClass &x : b->classes)
+      if (b->members[(size_t)x.idx[0]]->n == c->n) k = &x;
+    if (!k) {
+      b->classes.emplace_back();
+      k = &b->classes.back();
+    }
+    k->idx.push_back((int)i);
+  }
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  for (BatchClass &k : b->classes) {
+    const ll_ctx *c0 = b->members[(size_t)k.idx[0]];
+    const Shape &s = c0->shape;
+    k.st = s.st;
+    k.sw = s.sw;
+    k.tall_units = tall_grid(s);
+    k.wide_units = s.H / s.G;
+    k.T1 = s.T1;
+    k.T2 = s.T2;
+    k.smem_t = shape_tall_smem(s);
+    k.smem_w = shape_wide_smem(s);
+    std::vector<TallArgs> ta;
+    std::vector<WideArgs> wa;
+    for (int i : k.idx) {
+      ta.push_back(b->members[(size_t)i]->ta);
+      wa.push_back(b->members[(size_t)i]->wa);
+    }
+    if (upload(&k.d_ta, ta) != cudaSuccess || upload(&k.d_wa, wa) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&k.stream, cudaStreamNonBlocking) != cudaSuccess)
+      return LL_ERR_CUDA;
+    // chained launches when both passes of the class run in a few waves
+    int bw = 0, bt = 0;
+    const long long m = (long long)k.idx.size();
+    if (sms > 0 &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bw, k.sw->iter_batch, k.T1, k.smem_w) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, k.st->batch, k.T2, k.smem_t) == cudaSuccess && bw > 0 &&
+        bt > 0) {
+      const long long ww = (m * k.wide_units + (long long)sms * bw - 1) / ((long long)sms * bw);
+      const long long wt = (m * k.tall_units + (long long)sms * bt - 1) / ((long long)sms * bt);
+      k.pdl = ww <= 4 && wt <= 4;
+    }
+  }
+  return LL_OK;
+}
+
+static void launch_class(const void *kern, const void *arr, int units, int count, int threads, size_t smem,
+                         cudaStream_t st, bool chained) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(units * count));
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = chained ? 1 : 0;
+  void *argv[] = {(void *)&arr, (void *)&units};
+  cudaLaunchKernelExC(&cfg, kern, argv);
 }
 
 extern "C" {
@@ -1537,7 +1639,12 @@ ll_status ll_batch_create(int device, int32_t count, const uint32_t *q, const ui
     free_batch(b);
     return LL_ERR_CUDA;
   }
-  b->events.resize((size_t)count + 1, nullptr);
+  const ll_status cs = build_classes(b);
+  if (cs != LL_OK) {
+    free_batch(b);
+    return cs;
+  }
+  b->events.resize((size_t)count + b->classes.size() + 1, nullptr);
   for (auto &e : b->events)
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
       free_batch(b);
@@ -1578,8 +1685,25 @@ ll_status ll_batch_step(ll_batch *b, uint32_t iters, uint32_t flags, float *max_
     if (!b->graph_exec) {
       if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return LL_ERR_CUDA;
       cudaEventRecord(b->events[0], b->stream);
-      for (size_t i = 0; i < b->members.size(); ++i) {
-        ll_ctx *c = b->members[i];
+      size_t ev = 1;
+      std::vector<int> alone;
+      if (b->by_class) {
+        for (BatchClass &k : b->classes) {
+          cudaStreamWaitEvent(k.stream, b->events[0], 0);
+          const int m = (int)k.idx.size();
+          for (uint32_t it = 0; it < K; ++it) {
+            launch_class((const void *)k.st->batch, k.d_ta, k.tall_units, m, k.T2, k.smem_t, k.stream, it > 0 && k.pdl);
+            launch_class((const void *)k.sw->iter_batch, k.d_wa, k.wide_units, m, k.T1, k.smem_w, k.stream, k.pdl);
+          }
+          cudaEventRecord(b->events[ev], k.stream);
+          cudaStreamWaitEvent(b->stream, b->events[ev++], 0);
+        }
+        alone = b->singles;
+      } else {
+        for (size_t i = 0; i < b->members.size(); ++i) alone.push_back((int)i);
+      }
+      for (int i : alone) {
+        ll_ctx *c = b->members[(size_t)i];
         cudaStreamWaitEvent(c->stream, b->events[0], 0);
         const uint32_t off0 = c->offset;
         for (uint32_t k = 0; k < K; ++k) {
@@ -1587,8 +1711,8 @@ ll_status ll_batch_step(ll_batch *b, uint32_t iters, uint32_t flags, float *max_
           launch_wide(c, WIDE_ITER, true);
         }
         c->offset = off0;
-        cudaEventRecord(b->events[i + 1], c->stream);
-        cudaStreamWaitEvent(b->stream, b->events[i + 1], 0);
+        cudaEventRecord(b->events[ev], c->stream);
+        cudaStreamWaitEvent(b->stream, b->events[ev++], 0);
       }
       cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
       if (e != cudaSuccess) {
@@ -1629,6 +1753,15 @@ ll_status ll_batch_step(ll_batch *b, uint32_t iters, uint32_t flags, float *max_
 }
 
 void *ll_batch_stream(const ll_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+ll_status ll_batch_group_by_length(ll_batch *b, int32_t on) {
+  if (!b) return LL_ERR_ARG;
+  if (b->graph_exec) return LL_ERR_STATE;  // the step graph is captured on the first step
+  b->by_class = on != 0;
+  return LL_OK;
+}
+
+int32_t ll_batch_classes(const ll_batch *b) { return b ? (int32_t)b->classes.size() : 0; }
 
 ll_status ll_batch_sync(ll_batch *b) {
   if (!b) return LL_ERR_ARG;

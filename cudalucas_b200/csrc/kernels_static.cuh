@@ -268,7 +268,7 @@ __host__ __device__ constexpr int tall_extra() {
 // the partner's results back into the partner's slots.  (CTA 0 holds the
 // self-paired columns 0 and W/2 and always pairs through shared memory.)
 template <class P>
-__global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>())) tall_static(TallArgs a) {
+__device__ __forceinline__ void tall_body(const TallArgs &a, int blk) {
   constexpr int H = P::L, TR = H / 16, T = 2 * TR, CS = col_slots<H>();
   constexpr bool kHalf = tall_half_exchange<P>();
   static_assert((P::N == 2 || P::N == 3) && P::a[0] == 16 && P::a[P::N - 1] == 16, "radix list 16, (M,) 16");
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
   double2 *fr = pj + 8;              // w_H^(r*TR), half exchange
   double2 *sbase = fr + 16;          // per thread: w_N^(k1*t), half exchange
   double2 *spair = sbase + T;        // per thread: w_N^kA * w_H^tA, half exchange
-  const int c = blockIdx.x;
+  const int c = blk;
   const int W = a.W;
   const bool special = (c == 0);
   const int kA = special ? 0 : c;
@@ -406,6 +406,11 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
   for (int r = 0; r < 16; ++r) dst[t + r * TR] = cmulc(o[r], cmul(base, wr[col * 16 + r]));
 }
 
+template <class P>
+__global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>())) tall_static(TallArgs a) {
+  tall_body<P>(a, blockIdx.x);
+}
+
 // All stages of the radix list P in list order, in shared memory (Stockham:
 // natural order in and out); SIGN -1 with conjugate twiddles is the inverse
 // transform over the same twiddle table.
@@ -427,14 +432,14 @@ __device__ __forceinline__ void all_stages(double2 *s, const double2 *tw, int ro
 // arithmetic as the generic tall kernel, with every index and loop bound a
 // constant.
 template <class P, int TC, int PP>
-__global__ void __launch_bounds__(2 * PP * TC, min_blocks(2 * PP * TC)) tall_any(TallArgs a) {
+__device__ __forceinline__ void tall_any_body(const TallArgs &a, int blk) {
   constexpr int H = P::L, CS = col_slots<H>(), T = 2 * PP * TC;
   extern __shared__ double2 sm[];
   double2 *stw = sm + 2 * PP * CS;
   const int units = a.W / 2;
   const int col = threadIdx.x / TC, t = threadIdx.x - col * TC;  // col < 2*PP
   const int pl = col >> 1;
-  const int c = blockIdx.x * PP + pl;  // column pair
+  const int c = blk * PP + pl;  // column pair
   const bool active = c < units;
   const bool special = c == 0;
   const int W = a.W;
@@ -443,7 +448,7 @@ __global__ void __launch_bounds__(2 * PP * TC, min_blocks(2 * PP * TC)) tall_any
   for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
   griddep_wait();
   griddep_release();
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (blk == 0 && threadIdx.x == 0) {
     const uint32_t o = a.st->offset;  // CUDALucas.cu:1882, once per iteration
     a.st->offset = (uint32_t)((2ull * o) % a.q);
   }
@@ -489,6 +494,11 @@ __global__ void __launch_bounds__(2 * PP * TC, min_blocks(2 * PP * TC)) tall_any
   }
 }
 
+template <class P, int TC, int PP>
+__global__ void __launch_bounds__(2 * PP * TC, min_blocks(2 * PP * TC)) tall_any(TallArgs a) {
+  tall_any_body<P, TC, PP>(a, blockIdx.x);
+}
+
 template <class P, int G>
 constexpr int wide_threads() { return G * (P::L / 16); }
 
@@ -505,8 +515,9 @@ __device__ __forceinline__ double rnd_int(double x) {
 // stay below 2^53 and every scaling is by a power of two, so every step is
 // exact); carries are handed over as doubles, through shared memory between
 // the rows of a CTA and through global memory from CTA to CTA.
-template <class P, int G, int MODE>
-__global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<P, G>())) wide_static(WideArgs a) {
+// blk: the CTA's row group for WIDE_INIT (the iteration modes take tickets)
+template <class P, int G, int MODE, bool BATCH>
+__device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
   constexpr int W = P::L, TR = W / 16, T = G * TR;
   static_assert(P::a[0] == 16, "first radix must be 16");
   extern __shared__ double2 sm[];
@@ -517,7 +528,7 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   __shared__ uint32_t s_fault;
   if (threadIdx.x == 0) {
     s_fault = 0;
-    s_g = MODE == WIDE_INIT ? (int)blockIdx.x
+    s_g = MODE == WIDE_INIT ? (BATCH ? blk : (int)blockIdx.x)
                             : (int)(atomicAdd(&a.st->ticket, 1ull) % (unsigned long long)a.ngroups);
   }
   for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
@@ -727,3 +738,50 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
     }
   }
 }
+
+template <class P, int G, int MODE>
+__global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<P, G>())) wide_static(WideArgs a) {
+  wide_body<P, G, MODE, false>(a, 0);
+}
+
+// ---- batched launches: one launch runs a pass for every member of a length
+// class (members of one FFT length share the kernel); blockIdx.x = member *
+// units + unit.  A member's arguments are copied from the class's device
+// array into shared memory before anything else; they are constant for the
+// life of the batch, so this may overlap the previous pass (PDL).
+template <class Args>
+__device__ __forceinline__ const Args &member_args(const Args *arr, int m, Args *sa) {
+  static_assert(sizeof(Args) % 8 == 0, "copied as 64-bit words");
+  const uint64_t *src = reinterpret_cast<const uint64_t *>(&arr[m]);
+  uint64_t *dst = reinterpret_cast<uint64_t *>(sa);
+  for (int i = threadIdx.x; i < (int)(sizeof(Args) / 8); i += blockDim.x) dst[i] = __ldg(&src[i]);
+  __syncthreads();
+  return *sa;
+}
+
+template <class P>
+__global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>()))
+    tall_static_batch(const TallArgs *arr, int units) {
+  __shared__ __align__(16) TallArgs sa;
+  const int m = blockIdx.x / units;
+  const TallArgs &a = member_args(arr, m, &sa);
+  tall_body<P>(a, blockIdx.x - m * units);
+}
+
+template <class P, int TC, int PP>
+__global__ void __launch_bounds__(2 * PP * TC, min_blocks(2 * PP * TC)) tall_any_batch(const TallArgs *arr, int units) {
+  __shared__ __align__(16) TallArgs sa;
+  const int m = blockIdx.x / units;
+  const TallArgs &a = member_args(arr, m, &sa);
+  tall_any_body<P, TC, PP>(a, blockIdx.x - m * units);
+}
+
+template <class P, int G>
+__global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<P, G>()))
+    wide_static_batch(const WideArgs *arr, int units) {
+  __shared__ __align__(16) WideArgs sa;
+  const int m = blockIdx.x / units;
+  const WideArgs &a = member_args(arr, m, &sa);
+  wide_body<P, G, WIDE_ITER, true>(a, blockIdx.x - m * units);
+}
+

@@ -75,6 +75,8 @@ def lib():
         "ll_batch_step": (i32, [vp, u32, u32, fp]),
         "ll_batch_sync": (i32, [vp]),
         "ll_batch_stream": (vp, [vp]),
+        "ll_batch_group_by_length": (i32, [vp, i32]),
+        "ll_batch_classes": (i32, [vp]),
         "ll_batch_res64": (i32, [vp, ctypes.POINTER(u64)]),
         "ll_digits_res64": (u64, [i32p, u32, u32, u32]),
         "ll_digits_standardize": (i32, [i32p, u32, u32]),

@@ -153,6 +153,14 @@ ll_status ll_batch_start(ll_batch *b, const uint32_t *offsets);
 ll_status ll_batch_step(ll_batch *b, uint32_t iters, uint32_t flags, float *max_err);
 ll_status ll_batch_sync(ll_batch *b);
 void *ll_batch_stream(const ll_batch *b);  /* stream the step graphs run on */
+/* Members of one FFT length whose passes have specialised kernels form a
+ * length class: by default one launch per pass runs the pass for every
+ * member of the class (the graph then has one branch per class, 2 kernel
+ * nodes per iteration).  on = 0 launches every member's passes separately
+ * (one branch per member); call before the first ll_batch_step.
+ * ll_batch_classes gives the number of length classes. */
+ll_status ll_batch_group_by_length(ll_batch *b, int32_t on);
+int32_t ll_batch_classes(const ll_batch *b);
 ll_status ll_batch_res64(ll_batch *b, uint64_t *res64);
 
 /* Allocation-free LL steps.  No counterpart in the reference: CUDALucas

@@ -30,7 +30,7 @@ def large_entries():
 def reference_run_entries():
     """Res64 values printed by the reference binary itself on a B200."""
     out = []
-    for name in ("ref_c2_res64.json", "ref_c3_res64.json"):
+    for name in ("ref_c1_res64.json", "ref_c2_res64.json", "ref_c3_res64.json"):
         d = json.load(open(os.path.join(HERE, name)))
         out += [(p, k, int(r, 16)) for p, k, r in d["entries"]]
     return out

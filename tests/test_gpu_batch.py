@@ -35,6 +35,24 @@ def test_batch_equals_solo_and_exact():
         assert r == exact.res64(q, k), q
 
 
+@pytest.mark.parametrize("by_length", [True, False])
+def test_batch_length_classes_equal_solo(by_length):
+    """Members of equal length launched together per pass (one launch per
+    class) or separately give the solo residues."""
+    mix = [(86243, 4096), (86249, 4096), (1257787, 65536), (1257827, 65536), (1257859, 65536),
+           (216091, 12288), (216103, 12288), (2976221, 163840)]
+    qs, ns = zip(*mix)
+    offs = [(q * 5) // 9 for q in qs]
+    with cl.LLBatch(qs, ns, graph_iters=8, by_length=by_length) as b:
+        if by_length:
+            assert b.classes >= 2
+        b.start(offs)
+        b.step(83, report=True)
+        got = b.res64()
+    for (q, n), o, r in zip(mix, offs, got):
+        assert r == solo(q, n, o, 83), q
+
+
 def test_batch_steps_compose():
     qs, ns = zip(*MIX[:3])
     with cl.LLBatch(qs, ns, graph_iters=8) as b:

@@ -106,7 +106,12 @@ def test_selftest_long_table(p, r):
 
 
 def test_c1_full_test_216091_is_prime():
+    """C1: the whole test at 12K; Res64 at every 10000 equals the reference
+    binary's report lines (CUDALucas -f 12K -x 10000 216091), the final
+    residue is 0."""
     q, n = 216091, 12288
+    ref = {k: r for p, k, r in reference_run_entries() if p == q}
+    assert len(ref) == 21
     with cl.LLContext(q, n) as c:
         c.start(0)
         done, maxerr = 0, 0.0
@@ -114,6 +119,8 @@ def test_c1_full_test_216091_is_prime():
             k = min(10000, q - 2 - done)
             maxerr = max(maxerr, c.step(k, report=True))
             done += k
+            if done in ref:
+                assert c.res64() == ref[done], done
             if done == 10000:
                 assert c.res64() == KAT[q]
         assert c.res64() == 0
@@ -121,8 +128,11 @@ def test_c1_full_test_216091_is_prime():
 
 
 def test_c2_3200k_matches_exact_kat_and_reference_binary():
+    """C2: Res64 at every 10000 through 110000 equals the reference binary's
+    (CUDALucas -f 3200K -x 10000 57885161), and the exact values at 1..1000."""
     q, n = 57885161, 3276800
-    checks = {k: r for p, k, r in large_entries() + reference_run_entries() if p == q}
+    checks = {k: r for p, k, r in large_entries() + reference_run_entries() if p == q and k <= 110000}
+    assert all(k in checks for k in range(10000, 110001, 10000))
     with cl.LLContext(q, n) as c:
         c.start(0)
         done = 0
