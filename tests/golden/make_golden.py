@@ -7,7 +7,8 @@ CUDALucas.cu:2673-2729 (tables `tests[20]` and `testl[92]`).
 exact_res64.json: Res64 after k iterations for a spread of exponents and k,
 computed with exact big-integer arithmetic (oracle/exact.py).
 
-Run from the repository root:  python tests/golden/make_golden.py [REFDIR]
+Run from the repository root:  python tests/golden/make_golden.py REFDIR
+(REFDIR: the CUDALucas source tree; or set CUDALUCAS_SRC)
 """
 import json
 import os
@@ -56,7 +57,9 @@ def exact_table():
 
 
 if __name__ == "__main__":
-    refdir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    refdir = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CUDALUCAS_SRC")
+    if not refdir:
+        sys.exit("usage: make_golden.py REFDIR (the CUDALucas source tree), or set CUDALUCAS_SRC")
     kats = extract_kats(refdir)
     with open(os.path.join(HERE, "kat_res64.json"), "w") as f:
         json.dump(kats, f, indent=1)
