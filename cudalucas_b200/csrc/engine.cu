@@ -59,7 +59,9 @@ struct DevState {
   uint32_t offset;            // shift of the current state (doubled by tall pass)
   uint32_t err_bits;          // max roundoff error (float bits), reset by host
   uint32_t fault;             // bit 0: wait timeout, bit 1: carry overflow
-  uint32_t pad_[3];
+  uint32_t bar_count;         // grid barrier of the fused kernel: arrivals
+  uint32_t bar_gen;           //   and generation
+  uint32_t pad_;
 };
 
 struct TallArgs {
@@ -478,11 +480,33 @@ static const StaticTall kTall[] = {
     LLB_TALL_ANY(C1568, 112, 1),   LLB_TALL_ANY(C2744, 196, 1),
 };
 
-static const StaticWide *find_wide(int L) {
-  for (const auto &k : kWide)
-    if (k.L == L) return &k;
+// Fused cooperative kernels (fused_iters) for short lengths: the shape
+// (row length W, column length H) they are compiled for.  The tall pass uses
+// fewer column pairs per CTA than the two-launch kernels, for more CTAs.
+struct FusedKernel {
+  int W, H;
+  void (*run)(TallArgs, WideArgs, uint32_t, int);
+  int threads;      // per CTA
+  int tall_ppc;     // column pairs per tall unit
+  int smem;         // dynamic shared-memory entries
+};
+#define LLB_FUSED(LW, G, LT, TC, PP)                                                                        \
+  {LW::L, LT::L, fused_iters<LW, G, FusedTall<LT, TC, PP>>, fused_threads<LW, G, FusedTall<LT, TC, PP>>(), \
+   TC ? PP : 1,                                                                                              \
+   std::max(G * row_slots<LW::L, G>() + tw_size<LW>(),                                                     \
+            TC ? 2 * PP * col_slots<LT::L>() + tw_size<LT>() : padded(2 * LT::L) + tall_extra<LT>())}
+static const FusedKernel kFused[] = {
+    LLB_FUSED(L256, 4, C24, 2, 16),
+    LLB_FUSED(L256, 4, C28, 2, 16),
+    LLB_FUSED(L256, 4, C112, 8, 4),
+    LLB_FUSED(L256, 4, L256, 0, 1),
+};
+static const FusedKernel *find_fused(int W, int H) {
+  for (const auto &k : kFused)
+    if (k.W == W && k.H == H) return &k;
   return nullptr;
 }
+
 static const StaticTall *find_tall(int L) {
   for (const auto &k : kTall)
     if (k.L == L) return &k;
@@ -584,7 +608,7 @@ bool shape_ok(long long N, int W, int G, Shape &s) {
 bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
   if (N % 2 || !seven_smooth(N)) return false;
   // compile-time specialised kernels for both passes, W closest to sqrt(N)
-  if (!(t && (t->rows_per_cta > 0 || t->threads_wide > 0 || t->threads_tall > 0 || t->reserved[0]))) {
+  if (!(t && (t->rows_per_cta > 0 || t->threads_wide > 0 || t->threads_tall > 0 || (t->kernels & LL_KERNELS_GENERIC)))) {
     const StaticWide *bw = nullptr;
     const StaticTall *bt = nullptr;
     double best = 1e30;
@@ -720,6 +744,8 @@ struct ll_ctx {
   bool started = false;
   int inject = 0;
   bool pdl = false;  // chain the passes with programmatic dependent launch
+  const FusedKernel *fused = nullptr;  // iterations as one cooperative launch
+  int fused_grid = 0;
   float pending_err = 0.f;
   std::string err;
   TallArgs ta{};
@@ -925,6 +951,24 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
         ctx->pdl = ww <= 4 && wt <= 4;
       }
     }
+    // Short lengths with a fused kernel run their plain iterations as one
+    // cooperative launch, when all its CTAs fit on the GPU at once.
+    if (s.sw && s.st && !(tuning && (tuning->kernels & LL_KERNELS_NO_FUSED))) {
+      const FusedKernel *f = find_fused(s.W, s.H);
+      int sms = 0, per_sm = 0, coop = 0;
+      if (f && cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess && coop &&
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+          cudaFuncSetAttribute(f->run, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(sizeof(double2) * (size_t)f->smem)) == cudaSuccess &&
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f->run, f->threads,
+                                                        sizeof(double2) * (size_t)f->smem) == cudaSuccess) {
+        const int units = std::max((s.W / 2 + f->tall_ppc - 1) / f->tall_ppc, s.H / s.G);
+        if (per_sm > 0 && units <= sms * per_sm) {
+          ctx->fused = f;
+          ctx->fused_grid = units;
+        }
+      }
+    }
     TallArgs &ta = ctx->ta;
     ta.A = ctx->A; ta.stw = ctx->stwH; ta.twH = ctx->twH; ta.thi = ctx->thi; ta.tlo = ctx->tlo; ta.st = ctx->st;
     ta.ph = ctx->ph; ta.W = s.W; ta.H = s.H; ta.N = ctx->N; ta.ts = ctx->ts; ta.tmask = (1 << ctx->ts) - 1; ta.q = q;
@@ -1044,6 +1088,31 @@ static ll_status launch_iteration(ll_ctx *ctx, bool report) {
   return LL_OK;
 }
 
+// Plain iterations as fused cooperative launches (at most 4096 per launch).
+static ll_status launch_fused(ll_ctx *ctx, uint32_t iters) {
+  const FusedKernel *f = ctx->fused;
+  const Shape &s = ctx->shape;
+  int tall_units = (s.W / 2 + f->tall_ppc - 1) / f->tall_ppc;
+  for (uint32_t done = 0; done < iters;) {
+    uint32_t k = std::min<uint32_t>(iters - done, 4096u);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctx->fused_grid);
+    cfg.blockDim = dim3((unsigned)f->threads);
+    cfg.dynamicSmemBytes = sizeof(double2) * (size_t)f->smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *argv[] = {(void *)&ctx->ta, (void *)&ctx->wa, (void *)&k, (void *)&tall_units};
+    CK(cudaLaunchKernelExC(&cfg, (const void *)f->run, argv));
+    for (uint32_t i = 0; i < k; ++i) ctx->offset = (uint32_t)((2ull * ctx->offset) % ctx->q);
+    done += k;
+  }
+  return LL_OK;
+}
+
 ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
   if (!ctx) return LL_ERR_ARG;
   if (!ctx->started) return LL_ERR_STATE;
@@ -1056,7 +1125,13 @@ ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
   const bool report = (flags & LL_REPORT) != 0;
   uint32_t done = 0;
   const uint32_t K = (uint32_t)ctx->graph_iters;
-  if (K && iters >= K + (report ? 1u : 0u)) {
+  if (ctx->fused && iters >= 2u + (report ? 1u : 0u)) {
+    // plain iterations fused; the report iteration (if any) as two passes
+    const uint32_t plain = iters - (report ? 1u : 0u);
+    const ll_status rc = launch_fused(ctx, plain);
+    if (rc != LL_OK) return rc;
+    done = plain;
+  } else if (K && iters >= K + (report ? 1u : 0u)) {
     // iterations without a report, K at a time, replayed from one CUDA graph
     if (!ctx->graph_exec) {
       CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -1209,7 +1284,7 @@ void ll_shape(const ll_ctx *ctx, int32_t *width, int32_t *height, int32_t *rows_
 const char *ll_last_error(const ll_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 int32_t ll_kernel_kinds(const ll_ctx *ctx) {
   if (!ctx) return 0;
-  return (ctx->shape.sw ? 1 : 0) | (ctx->shape.st ? 2 : 0);
+  return (ctx->shape.sw ? 1 : 0) | (ctx->shape.st ? 2 : 0) | (ctx->fused ? 4 : 0);
 }
 void ll_debug_inject_failure(ll_ctx *ctx, int32_t count) {
   if (ctx) ctx->inject = count;
@@ -1625,6 +1700,7 @@ ll_status ll_batch_create(int device, int32_t count, const uint32_t *q, const ui
   b->graph_iters = graph_iters > 0 ? graph_iters : 10;
   ll_tuning t{};
   t.graph_iters = -1;  // members never capture their own graphs
+  t.kernels = LL_KERNELS_NO_FUSED;  // members run in the batch's graph
   for (int32_t i = 0; i < count; ++i) {
     ll_ctx *c = nullptr;
     ll_status s = ll_create(device, q[i], n[i], &t, &c);

@@ -112,12 +112,25 @@ __host__ __device__ constexpr int row_slots() {
   return L + L / 16 + (G > 1 ? ((8 / G - (L + L / 16) % 8) % 8 + 8) % 8 : 0);
 }
 
+// Barriers of the kernel bodies: the whole CTA (__syncthreads), or the first
+// n threads of the CTA (named barrier `id`), which lets a body run on a part
+// of a larger CTA.
+struct CtaSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+struct PartSync {
+  int id, n;
+  __device__ __forceinline__ void operator()() const {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+  }
+};
+
 // One Stockham stage of every row of the CTA, in place in shared memory.
 // Thread t of a row handles butterflies t, t+TR, ... (a guard skips the
 // tail when L/R is not a multiple of TR).  `tw` points at this stage's
 // twiddle block (NS rows of R-1 entries) in shared memory.
-template <int L, int RS, int R, int NS, int SIGN, int TR>
-__device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, int t) {
+template <int L, int RS, int R, int NS, int SIGN, int TR, class S = CtaSync>
+__device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, int t, S sync = S()) {
   const int rb = row * RS;
   constexpr int M = L / R;
   constexpr int NB = (M + TR - 1) / TR;
@@ -150,7 +163,7 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, i
   }
   // with one butterfly per thread and NS == L/R a thread stores exactly the
   // slots it loaded: no barrier between the loads and the stores
-  if constexpr (!(NB == 1 && NS == M)) __syncthreads();
+  if constexpr (!(NB == 1 && NS == M)) sync();
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const int j = t + b * TR;
@@ -161,27 +174,27 @@ __device__ __forceinline__ void sstage(double2 *s, const double2 *tw, int row, i
       for (int r = 0; r < R; ++r) s[rb + pad(ob + r * NS)] = v[b][sslot<R>(r)];
     }
   }
-  __syncthreads();
+  sync();
 }
 
 // forward stages [I, E) (radix a[I], NS = a[0]*...*a[I-1])
-template <class P, int RS, int I, int E, int NS, int TR>
-__device__ __forceinline__ void fwd_stages(double2 *s, const double2 *tw, int row, int t) {
+template <class P, int RS, int I, int E, int NS, int TR, class S = CtaSync>
+__device__ __forceinline__ void fwd_stages(double2 *s, const double2 *tw, int row, int t, S sync = S()) {
   if constexpr (I < E) {
     constexpr int R = P::a[I];
-    sstage<P::L, RS, R, NS, +1, TR>(s, tw + tw_offset<P, I>(), row, t);
-    fwd_stages<P, RS, I + 1, E, NS * R, TR>(s, tw, row, t);
+    sstage<P::L, RS, R, NS, +1, TR>(s, tw + tw_offset<P, I>(), row, t, sync);
+    fwd_stages<P, RS, I + 1, E, NS * R, TR>(s, tw, row, t, sync);
   }
 }
 
 // inverse stages [I, E) of the reversed list (radix a[N-1-I])
-template <class P, int RS, int I, int E, int NS, int TR>
-__device__ __forceinline__ void inv_stages(double2 *s, const double2 *tw, int row, int t) {
+template <class P, int RS, int I, int E, int NS, int TR, class S = CtaSync>
+__device__ __forceinline__ void inv_stages(double2 *s, const double2 *tw, int row, int t, S sync = S()) {
   static_assert(palindromic<P>(), "inverse stages reuse the forward twiddle table");
   if constexpr (I < E) {
     constexpr int R = P::a[P::N - 1 - I];
-    sstage<P::L, RS, R, NS, -1, TR>(s, tw + tw_offset<P, I>(), row, t);
-    inv_stages<P, RS, I + 1, E, NS * R, TR>(s, tw, row, t);
+    sstage<P::L, RS, R, NS, -1, TR>(s, tw + tw_offset<P, I>(), row, t, sync);
+    inv_stages<P, RS, I + 1, E, NS * R, TR>(s, tw, row, t, sync);
   }
 }
 
@@ -267,8 +280,8 @@ __host__ __device__ constexpr int tall_extra() {
 // mirror bins, r >= 8 of the partner, come through shared memory) and writes
 // the partner's results back into the partner's slots.  (CTA 0 holds the
 // self-paired columns 0 and W/2 and always pairs through shared memory.)
-template <class P>
-__device__ __forceinline__ void tall_body(const TallArgs &a, int blk) {
+template <class P, class S = CtaSync>
+__device__ __forceinline__ void tall_body(const TallArgs &a, int blk, S sync = S()) {
   constexpr int H = P::L, TR = H / 16, T = 2 * TR, CS = col_slots<H>();
   constexpr bool kHalf = tall_half_exchange<P>();
   static_assert((P::N == 2 || P::N == 3) && P::a[0] == 16 && P::a[P::N - 1] == 16, "radix list 16, (M,) 16");
@@ -317,21 +330,21 @@ __device__ __forceinline__ void tall_body(const TallArgs &a, int blk) {
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = src[t + r * TR];
     cp_async_wait_all();
-    __syncthreads();
+    sync();
     if constexpr (kHalf) base = sbase[threadIdx.x];
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = cmul(v[r], cmul(base, wr[col * 16 + r]));
     first_stage_from_regs<H, CS, TR>(sm, v, col, t);
   }
-  __syncthreads();
-  fwd_stages<P, CS, 1, P::N - 1, 16, TR>(sm, stw, col, t);
+  sync();
+  fwd_stages<P, CS, 1, P::N - 1, 16, TR>(sm, stw, col, t, sync);
   double2 o[16];
   last_stage_to_regs<H, CS, TR, +1>(sm, stw + tw_offset<P, P::N - 1>(), o, col, t);
   double2 *own = sm + col * CS;  // own bin r: own[pad(t + r*TR)]
   if (kHalf && !special) {
 #pragma unroll
     for (int r = 8; r < 16; ++r) own[pad(t + r * TR)] = o[r];
-    __syncthreads();
+    sync();
     double2 *mir = sm + (col ^ 1) * CS;  // partner's bin 15-r: mir[pad(TR-1-t + (15-r)*TR)]
     // Swapping the two bins and conjugating w swaps the two results of
     // pair_square, so both columns make the same call: column kB passes its
@@ -347,13 +360,13 @@ __device__ __forceinline__ void tall_body(const TallArgs &a, int blk) {
       pair_square(o[r], zm, w);
       mir[ps] = zm;
     }
-    __syncthreads();
+    sync();
 #pragma unroll
     for (int r = 8; r < 16; ++r) o[r] = own[pad(t + r * TR)];
   } else {
 #pragma unroll
     for (int r = 0; r < 16; ++r) own[pad(t + r * TR)] = o[r];
-    __syncthreads();
+    sync();
     // pairing by index: i = threadIdx.x + j*T, w_H^i = w_H^threadIdx.x * pj[j]
     const double2 wt = __ldg(&a.twH[threadIdx.x]);
     if (!special) {
@@ -391,14 +404,14 @@ __device__ __forceinline__ void tall_body(const TallArgs &a, int blk) {
         }
       }
     }
-    __syncthreads();
+    sync();
 #pragma unroll
     for (int r = 0; r < 16; ++r) o[r] = own[pad(t + r * TR)];
   }
-  __syncthreads();  // every thread's slot reads are done before the stage-0 stores
+  sync();  // every thread's slot reads are done before the stage-0 stores
   first_stage_from_regs<H, CS, TR, -1>(sm, o, col, t);
-  __syncthreads();
-  inv_stages<P, CS, 1, P::N - 1, 16, TR>(sm, stw, col, t);
+  sync();
+  inv_stages<P, CS, 1, P::N - 1, 16, TR>(sm, stw, col, t, sync);
   last_stage_to_regs<H, CS, TR>(sm, stw + tw_offset<P, P::N - 1>(), o, col, t);
   double2 *dst = a.A + (size_t)k1 * H;
   if constexpr (kHalf) base = sbase[threadIdx.x];
@@ -414,12 +427,12 @@ __global__ void __launch_bounds__(tall_threads<P>(), min_blocks(tall_threads<P>(
 // All stages of the radix list P in list order, in shared memory (Stockham:
 // natural order in and out); SIGN -1 with conjugate twiddles is the inverse
 // transform over the same twiddle table.
-template <class P, int RS, int I, int NS, int TR, int SIGN>
-__device__ __forceinline__ void all_stages(double2 *s, const double2 *tw, int row, int t) {
+template <class P, int RS, int I, int NS, int TR, int SIGN, class S = CtaSync>
+__device__ __forceinline__ void all_stages(double2 *s, const double2 *tw, int row, int t, S sync = S()) {
   if constexpr (I < P::N) {
     constexpr int R = P::a[I];
-    sstage<P::L, RS, R, NS, SIGN, TR>(s, tw + tw_offset<P, I>(), row, t);
-    all_stages<P, RS, I + 1, NS * R, TR, SIGN>(s, tw, row, t);
+    sstage<P::L, RS, R, NS, SIGN, TR>(s, tw + tw_offset<P, I>(), row, t, sync);
+    all_stages<P, RS, I + 1, NS * R, TR, SIGN>(s, tw, row, t, sync);
   }
 }
 
@@ -431,8 +444,8 @@ __device__ __forceinline__ void all_stages(double2 *s, const double2 *tw, int ro
 // with conjugate twiddles and stored with the conjugate twiddle.  The same
 // arithmetic as the generic tall kernel, with every index and loop bound a
 // constant.
-template <class P, int TC, int PP>
-__device__ __forceinline__ void tall_any_body(const TallArgs &a, int blk) {
+template <class P, int TC, int PP, class S = CtaSync>
+__device__ __forceinline__ void tall_any_body(const TallArgs &a, int blk, S sync = S()) {
   constexpr int H = P::L, CS = col_slots<H>(), T = 2 * PP * TC;
   extern __shared__ double2 sm[];
   double2 *stw = sm + 2 * PP * CS;
@@ -458,8 +471,8 @@ __device__ __forceinline__ void tall_any_body(const TallArgs &a, int blk) {
     for (int m2 = t; m2 < H; m2 += TC) row[pad(m2)] = cmul(src[m2], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
   }
   cp_async_wait_all();
-  __syncthreads();
-  all_stages<P, CS, 0, 1, TC, +1>(sm, stw, col, t);
+  sync();
+  all_stages<P, CS, 0, 1, TC, +1>(sm, stw, col, t, sync);
   if (active) {
     const int ti = threadIdx.x - 2 * pl * TC;  // thread of the pair, < 2*TC
     double2 *ra = sm + 2 * pl * CS, *rb = ra + CS;
@@ -486,8 +499,8 @@ __device__ __forceinline__ void tall_any_body(const TallArgs &a, int blk) {
       }
     }
   }
-  __syncthreads();
-  all_stages<P, CS, 0, 1, TC, -1>(sm, stw, col, t);
+  sync();
+  all_stages<P, CS, 0, 1, TC, -1>(sm, stw, col, t, sync);
   if (active) {
     double2 *dst = a.A + (size_t)k1 * H;
     for (int m2 = t; m2 < H; m2 += TC) dst[m2] = cmulc(row[pad(m2)], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
@@ -500,7 +513,7 @@ __global__ void __launch_bounds__(2 * PP * TC, min_blocks(2 * PP * TC)) tall_any
 }
 
 template <class P, int G>
-constexpr int wide_threads() { return G * (P::L / 16); }
+__host__ __device__ constexpr int wide_threads() { return G * (P::L / 16); }
 
 // Nearest integer of x for |x| < 2^51 (ties to even) by adding and removing
 // 1.5*2^52: two FP64 adds instead of a rounding instruction.  The _rn
@@ -516,8 +529,8 @@ __device__ __forceinline__ double rnd_int(double x) {
 // exact); carries are handed over as doubles, through shared memory between
 // the rows of a CTA and through global memory from CTA to CTA.
 // blk: the CTA's row group for WIDE_INIT (the iteration modes take tickets)
-template <class P, int G, int MODE, bool BATCH>
-__device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
+template <class P, int G, int MODE, bool BATCH, class S = CtaSync>
+__device__ __forceinline__ void wide_body(const WideArgs &a, int blk, S sync = S()) {
   constexpr int W = P::L, TR = W / 16, T = G * TR;
   static_assert(P::a[0] == 16, "first radix must be 16");
   extern __shared__ double2 sm[];
@@ -532,7 +545,7 @@ __device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
                             : (int)(atomicAdd(&a.st->ticket, 1ull) % (unsigned long long)a.ngroups);
   }
   for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
-  __syncthreads();
+  sync();
   const int g = s_g;
   const int H = a.H;
   const int m2b = g * G;
@@ -596,12 +609,12 @@ __device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
     }
     const bool w_sub = dw & 1;
     cp_async_wait_all();
-    __syncthreads();
-    if constexpr (kDirect) inv_stages<P, RS, 1, P::N - 1, 16, TR>(sm, stw, row, t);
-    else inv_stages<P, RS, 0, P::N - 1, 1, TR>(sm, stw, row, t);
+    sync();
+    if constexpr (kDirect) inv_stages<P, RS, 1, P::N - 1, 16, TR>(sm, stw, row, t, sync);
+    else inv_stages<P, RS, 0, P::N - 1, 1, TR>(sm, stw, row, t, sync);
     double2 u[16];
     last_stage_to_regs<W, RS, TR>(sm, stw + tw_offset<P, P::N - 1>(), u, row, t);
-    __syncthreads();  // shared memory is reused for the carry hand-off below
+    sync();  // shared memory is reused for the carry hand-off below
 
     // Carry in FP64 only (no integer conversions).  Phase 1 leaves, in the
     // shared-memory slot of element (row, m1), the packed pair
@@ -662,7 +675,7 @@ __device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
       }
       __syncwarp();
     } else {
-      __syncthreads();
+      sync();
       if (threadIdx.x == 0) {
         for (int w = 0; w < NW; ++w) {
           uint32_t *f = &a.flags[pred * kWarpFlags + w];
@@ -670,7 +683,7 @@ __device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
           *f = 0;
         }
       }
-      __syncthreads();
+      sync();
     }
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
@@ -695,10 +708,10 @@ __device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
       }
       x[r] = make_double2(d0 * (W0 * (n0 ? a.colS2[r] : a.colS[r])), d1 * (W1 * (n1 ? a.colS2[r] : a.colS[r])));
     }
-    __syncthreads();  // carry reads done before the data region is rewritten
+    sync();  // carry reads done before the data region is rewritten
   } else {
     cp_async_wait_all();
-    __syncthreads();
+    sync();
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m1 = t + r * TR;
@@ -710,9 +723,9 @@ __device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
     }
   }
   first_stage_from_regs<W, RS, TR>(sm, x, row, t);
-  __syncthreads();
+  sync();
   if constexpr (kDirect) {
-    fwd_stages<P, RS, 1, P::N - 1, 16, TR>(sm, stw, row, t);
+    fwd_stages<P, RS, 1, P::N - 1, 16, TR>(sm, stw, row, t, sync);
     // the last stage (radix 16) leaves elements t + r*TR in registers: store
     // them straight to global memory
     last_stage_to_regs<W, RS, TR, +1>(sm, stw + tw_offset<P, P::N - 1>(), x, row, t);
@@ -720,7 +733,7 @@ __device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
 #pragma unroll
     for (int r = 0; r < 16; ++r) dst[(size_t)(t + r * TR) * H] = x[r];
   } else {
-    fwd_stages<P, RS, 1, P::N, 16, TR>(sm, stw, row, t);
+    fwd_stages<P, RS, 1, P::N, 16, TR>(sm, stw, row, t, sync);
     for (int k1 = threadIdx.x; k1 < W; k1 += T) a.A[(size_t)k1 * H + m2b] = sm[pad(k1)];
   }
   if (MODE != WIDE_INIT) {
@@ -729,7 +742,7 @@ __device__ __forceinline__ void wide_body(const WideArgs &a, int blk) {
     for (int o = 16; o; o >>= 1) em = fmaxf(em, __shfl_xor_sync(0xffffffffu, em, o));
     if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = em;
     if (out_of_range) atomicOr(&s_fault, 2u);
-    __syncthreads();
+    sync();
     if (threadIdx.x == 0) {
       float m = 0.f;
       for (int i = 0; i < (T + 31) / 32; ++i) m = fmaxf(m, s_err[i]);
@@ -783,5 +796,86 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   const int m = blockIdx.x / units;
   const WideArgs &a = member_args(arr, m, &sa);
   wide_body<P, G, WIDE_ITER, true>(a, blockIdx.x - m * units);
+}
+
+// ---- fused iterations for short lengths ---------------------------------
+// One cooperative launch runs `iters` iterations: every CTA takes part in
+// both passes, looping over their units, and the passes are separated by
+// grid-wide barriers instead of kernel boundaries, so a length whose passes
+// are a few microseconds of work each no longer pays two launches per
+// iteration.  The block has max(T1, T2) threads; a pass whose CTA shape is
+// smaller runs on the first threads with a named barrier.
+
+// Grid-wide barrier (all CTAs are co-resident: cooperative launch).  The
+// fences around the arrival make every CTA's writes before the barrier
+// visible to every CTA's reads after it.  The wait is bounded: on expiry it
+// sets fault bit 0 and returns false.
+__device__ __forceinline__ bool grid_sync(DevState *st, unsigned nblocks) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned g;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(&st->bar_gen) : "memory");
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(&st->bar_count, 1u) == nblocks - 1) {
+      atomicExch(&st->bar_count, 0u);
+      __threadfence();
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&st->bar_gen), "r"(g + 1u) : "memory");
+    } else {
+      ok = 0;
+      for (int it = 0; it < (1 << 24); ++it) {
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(&st->bar_gen) : "memory");
+        if (v != g) {
+          ok = 1;
+          break;
+        }
+        __nanosleep(it < 64 ? 32 : 256);
+      }
+      if (!ok) atomicOr(&st->fault, 1u);
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Tall pass of the fused kernel: tall_body (TC == 0) or tall_any_body.
+template <class PT, int TC, int PP>
+struct FusedTall {
+  static constexpr int threads = TC ? 2 * PP * TC : tall_threads<PT>();
+  template <class S>
+  __device__ __forceinline__ static void run(const TallArgs &a, int u, S sync) {
+    if constexpr (TC) tall_any_body<PT, TC, PP, S>(a, u, sync);
+    else tall_body<PT, S>(a, u, sync);
+  }
+};
+
+template <class PW, int G, class TP>
+__host__ __device__ constexpr int fused_threads() {
+  return wide_threads<PW, G>() > TP::threads ? wide_threads<PW, G>() : TP::threads;
+}
+
+template <class PW, int G, class TP>
+__global__ void __launch_bounds__(fused_threads<PW, G, TP>(), 1)
+    fused_iters(TallArgs ta, WideArgs wa, uint32_t iters, int tall_units) {
+  constexpr int TPB = fused_threads<PW, G, TP>(), T1 = wide_threads<PW, G>(), T2 = TP::threads;
+  const int wide_units = wa.ngroups;
+  for (uint32_t it = 0; it < iters; ++it) {
+    for (int u = blockIdx.x; u < tall_units; u += gridDim.x) {
+      if constexpr (T2 == TPB) TP::run(ta, u, CtaSync());
+      else if (threadIdx.x < T2) TP::run(ta, u, PartSync{1, T2});
+      __syncthreads();  // the next unit reuses the shared memory
+    }
+    if (!grid_sync(ta.st, gridDim.x)) return;
+    for (int u = blockIdx.x; u < wide_units; u += gridDim.x) {
+      if constexpr (T1 == TPB) wide_body<PW, G, WIDE_ITER, false>(wa, u, CtaSync());
+      else if (threadIdx.x < T1) wide_body<PW, G, WIDE_ITER, false>(wa, u, PartSync{1, T1});
+      __syncthreads();
+    }
+    if (!grid_sync(ta.st, gridDim.x)) return;
+  }
 }
 

@@ -129,7 +129,7 @@ class LLContext:
         native.lib().ll_shape(self._h, *[ctypes.byref(x) for x in v])
         d = dict(zip(("W", "H", "G", "threads_wide", "threads_tall"), [x.value for x in v]))
         k = native.lib().ll_kernel_kinds(self._h)
-        d["wide_specialised"], d["tall_specialised"] = bool(k & 1), bool(k & 2)
+        d["wide_specialised"], d["tall_specialised"], d["fused"] = bool(k & 1), bool(k & 2), bool(k & 4)
         return d
 
 

@@ -21,12 +21,15 @@ LL_REPORT = 1
 LL_ERRCHK = 2
 LL_ASYNC = 4
 LL_STATIC_MAX_WORDS = 1 << 20
+LL_KERNELS_GENERIC = 1
+LL_KERNELS_NO_FUSED = 2
 
 
 class Tuning(ctypes.Structure):
     _fields_ = [("width", ctypes.c_int32), ("rows_per_cta", ctypes.c_int32),
                 ("threads_wide", ctypes.c_int32), ("threads_tall", ctypes.c_int32),
-                ("graph_iters", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+                ("graph_iters", ctypes.c_int32), ("kernels", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 2)]
 
 
 _lib = None

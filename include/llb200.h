@@ -53,8 +53,15 @@ typedef struct {
   int32_t threads_wide; /* threads per CTA of the wide pass                 */
   int32_t threads_tall; /* threads per CTA of the tall pass                 */
   int32_t graph_iters;  /* iterations captured per CUDA graph (0 = auto)    */
-  int32_t reserved[3];
+  int32_t kernels;      /* LL_KERNELS_* flags (0 = the engine's choice)     */
+  int32_t reserved[2];
 } ll_tuning;
+
+/* ll_tuning.kernels: LL_KERNELS_GENERIC forces the generic (runtime-plan)
+ * kernels; LL_KERNELS_NO_FUSED keeps short lengths on two launches per
+ * iteration instead of the fused cooperative kernel. */
+#define LL_KERNELS_GENERIC 1
+#define LL_KERNELS_NO_FUSED 2
 
 /* Creates a context for exponent q at FFT length n (FP64 words) on `device`.
  * Replaces alloc_gpu_mem + write_gpu_data (CUDALucas.cu:1096, :1125).
@@ -121,7 +128,8 @@ void ll_shape(const ll_ctx *ctx, int32_t *width, int32_t *height,
               int32_t *rows_per_cta, int32_t *threads_wide, int32_t *threads_tall);
 const char *ll_last_error(const ll_ctx *ctx); /* text of the last failure   */
 /* Which passes run compile-time specialised kernels: bit 0 the wide (row)
- * pass, bit 1 the tall (column) pass; the others use the generic kernels. */
+ * pass, bit 1 the tall (column) pass (the others use the generic kernels);
+ * bit 2: plain iterations run as fused cooperative launches. */
 int32_t ll_kernel_kinds(const ll_ctx *ctx);
 const char *ll_status_string(ll_status s);
 

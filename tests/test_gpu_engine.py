@@ -271,3 +271,19 @@ def test_specialised_columns_of_any_radix_list(nk):
         set_threads(1)
     assert cl.digits_res64(d, q, n, o_off) == want
     assert err < 0.4 and err <= 2 * oerr + 1e-3 and oerr <= 2 * err + 1e-3, (err, oerr)
+
+
+@pytest.mark.parametrize("n", [12288, 14336, 57344, 131072])
+def test_fused_iterations_equal_two_launch_iterations(n):
+    """Short lengths run their plain iterations as one cooperative launch
+    with grid barriers between the passes; the digits are bit for bit those
+    of two launches per iteration, and match the oracle's residue."""
+    off = q // 3
+    d1, o1, e1, s1 = engine_run(q, n, off, 700)
+    d2, o2, e2, s2 = engine_run(q, n, off, 700, kernels=cl.native.LL_KERNELS_NO_FUSED)
+    assert s1["fused"] and not s2["fused"], (s1, s2)
+    assert o1 == o2 and np.array_equal(d1, d2) and e1 == e2
+    o = Oracle(q, n)
+    o.start(off)
+    o.step(700)
+    assert cl.digits_res64(d1, q, n, o1) == o.res64()
