@@ -256,3 +256,29 @@ def test_checkpoint_written_by_llucas_resumes_in_the_reference(cli, tmp_path):
     r = subprocess.run([REF, str(q)], cwd=str(tmp_path), capture_output=True, text=True, timeout=300)
     assert "Continuing M%d @ iteration " % q in r.stdout, r.stdout[-2000:]
     assert "M( %d )P" % q in r.stdout, r.stdout[-2000:]
+
+
+@pytest.mark.gpu
+def test_cli_cufftbench_writes_the_gpu_tables_and_they_are_read(cli, tmp_path):
+    """-cufftbench s e passes (CUDALucas.cu:2413-2587): times the supported
+    lengths from s K to e K, writes `<gpu> fft.txt` in the reference's layout
+    (kept lengths only) and `<gpu> shapes.txt`; a later run reads fft.txt
+    (init_ffts, CUDALucas.cu:975-1021) and chooses from the kept lengths."""
+    import cudalucas_b200 as cl
+    (tmp_path / "CUDALucas.ini").write_text(INI)
+    r = run(cli, "-cufftbench", "12", "20", "2", cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    gpu = cl.device_name(0)
+    fft = (tmp_path / ("%s fft.txt" % gpu)).read_text().split("\n")
+    assert "  fft    max exp  ms/iter" in fft
+    rows = [l.split() for l in fft if l[:5].strip().isdigit()]
+    assert rows and all(12 <= int(k) <= 20 for k, _, _ in rows)
+    assert ["16" == k for k, _, _ in rows].count(True) == 1      # a power of two is always kept
+    shapes = (tmp_path / ("%s shapes.txt" % gpu)).read_text().split("\n")
+    assert any(l.split()[:1] == ["12"] for l in shapes if l and l[0] != "#")
+    kept = [int(k) for k, _, _ in rows]
+    # M216091's default length is 14K; with the table it is the smallest kept length >= its lower bound
+    want = min(k for k in kept if k * 1024 >= cl.fft_bounds(216091)[0])
+    (tmp_path / "CUDALucas.ini").write_text(INI.replace("ReportIterations=10000", "ReportIterations=100"))
+    rc, out, err = run_until([cli, "216091"], tmp_path, "Iteration 200 ")
+    assert "Starting M216091 fft length = %dK" % want in out, out[:500]
