@@ -394,6 +394,16 @@ def run_reference(args, world, rank, local):
                                     "program (cuFFT path on GPU %d); it has no host-core implementation"
                                     % (K, S, local)},
     })
+    # the reference's kernel-only timing of the same length (-cufftbench,
+    # CUDALucas.cu:2445-2490: cuFFT x2 + square + rcb + splice, no read-back)
+    try:
+        r = subprocess.run([exe, "-d", str(local), "-cufftbench", str(n // 1024), str(n // 1024), "20"], cwd=work,
+                           capture_output=True, text=True, timeout=300)
+        m = re.search(r"ave time = ([0-9.]+) msec", r.stdout)
+        base["kernel_only"] = {"value": float(m.group(1)) if m else None, "unit": "ms/iter",
+                               "command": "-cufftbench %d %d 20" % (n // 1024, n // 1024)}
+    except Exception as exc:
+        base["kernel_only"] = {"value": None, "error": str(exc)[:200]}
     return base
 
 
