@@ -282,3 +282,13 @@ def test_cli_cufftbench_writes_the_gpu_tables_and_they_are_read(cli, tmp_path):
     (tmp_path / "CUDALucas.ini").write_text(INI.replace("ReportIterations=10000", "ReportIterations=100"))
     rc, out, err = run_until([cli, "216091"], tmp_path, "Iteration 200 ")
     assert "Starting M216091 fft length = %dK" % want in out, out[:500]
+
+
+@pytest.mark.gpu
+@pytest.mark.slow
+def test_cli_long_selftest(cli, tmp_path):
+    """-r 1: the 92-entry table of CUDALucas.cu:2684-2729, 10000 iterations
+    each at the default length."""
+    r = subprocess.run([cli, "-r", "1"], cwd=str(tmp_path), capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-2000:]
+    assert r.stdout.count("This residue is correct.") == 92
