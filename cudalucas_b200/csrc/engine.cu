@@ -74,6 +74,7 @@ struct TallArgs {
   FftPlan ph;
   int W, H, N, ts, tmask;
   uint32_t q;
+  int pf;  // > 0: prefetch into L2 the column pair pf units ahead (state larger than L2)
 };
 
 // Ready flags per wide-pass CTA: the specialised kernels hand the carry over
@@ -96,6 +97,7 @@ struct WideArgs {
   DevState *st;
   FftPlan pw;
   int W, H, G, ngroups;
+  int pf;  // > 0: prefetch into L2 the row group pf tickets ahead (state larger than L2)
   uint32_t q, n, b, qn;
   // specialised kernels: column m1 = t + r*TR has exponent colF[t] - colD[r]
   // (mod n), i.e. weight colW[t] * colS[r] (times 2 when it wraps)
@@ -978,6 +980,21 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
     wa.colF = ctx->colF; wa.colW = ctx->colW; wa.colWi = ctx->colWi;
     wa.st = ctx->st; wa.pw = ctx->pw; wa.W = s.W; wa.H = s.H; wa.G = s.G; wa.ngroups = ngroups;
     wa.q = q; wa.n = n; wa.b = ctx->b; wa.qn = ctx->qn;
+    // A state larger than half of L2 is read from HBM by every pass: each CTA
+    // prefetches into L2 the unit about one wave ahead (the CTAs resident at
+    // once), so that unit's loads hit L2.
+    {
+      int l2 = 0, sms = 0, bw = 0, bt = 0;
+      const bool big = cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, device) == cudaSuccess &&
+                       16.0 * ctx->N > 0.5 * l2;
+      if (big && s.sw && s.st && !(tuning && (tuning->kernels & LL_KERNELS_NO_PREFETCH)) &&
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bw, s.sw->iter, s.T1, shape_wide_smem(s)) == cudaSuccess &&
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bt, s.st->run, s.T2, shape_tall_smem(s)) == cudaSuccess) {
+        if (s.W >= 2048) wa.pf = sms * bw;  // the kernels of shorter rows have no prefetch
+        if (s.st->ppc == 1 && s.H >= 2048) ta.pf = sms * bt;
+      }
+    }
     if (s.sw) {
       // column m1 = t + r*TR: exponent colF[t] - D_r (mod n), D_r = r*TR*2H*b mod n
       const long long TR = s.W / 16;

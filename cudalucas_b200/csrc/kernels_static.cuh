@@ -242,6 +242,17 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
 }
 
+// L2 prefetches: a contiguous range (bulk, 16-byte aligned, size a multiple
+// of 16) or one line.  When the state is larger than L2, a CTA prefetches the
+// data of the unit about one wave ahead while it computes, so that unit's
+// loads hit L2 instead of HBM.
+__device__ __forceinline__ void prefetch_l2_bulk(const void *p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+template <int L>
+constexpr bool kPrefetchRows = L >= 2048;
+
 // Programmatic dependent launch.  The passes are launched with programmatic
 // stream serialization, so a kernel may become resident while the previous
 // pass drains and run its prologue (tables, twiddles, ticket) early.
@@ -335,6 +346,11 @@ __device__ __forceinline__ void tall_body(const TallArgs &a, int blk, S sync = S
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = cmul(v[r], cmul(base, wr[col * 16 + r]));
     first_stage_from_regs<H, CS, TR>(sm, v, col, t);
+  }
+  if (kPrefetchRows<H> && a.pf && threadIdx.x == 0 && c + a.pf < W / 2) {
+    const int c2 = c + a.pf;  // never 0: the pair of columns c2 and W - c2
+    prefetch_l2_bulk(a.A + (size_t)c2 * H, H * (uint32_t)sizeof(double2));
+    prefetch_l2_bulk(a.A + (size_t)(W - c2) * H, H * (uint32_t)sizeof(double2));
   }
   sync();
   fwd_stages<P, CS, 1, P::N - 1, 16, TR>(sm, stw, col, t, sync);
@@ -594,6 +610,13 @@ __device__ __forceinline__ void wide_body(const WideArgs &a, int blk, S sync = S
       first_stage_from_regs<W, RS, TR, -1>(sm, v, row, t);
     } else {
       for (int k1 = threadIdx.x; k1 < W; k1 += T) cp_async16(&sm[pad(k1)], &a.A[(size_t)k1 * H + m2b]);
+    }
+    // (compiled for long rows only: only states larger than L2 prefetch, and
+    // those have rows of 2048 and more)
+    if (kPrefetchRows<W> && a.pf && g + a.pf < a.ngroups) {
+      const double2 *nxt = a.A + (size_t)(g + a.pf) * G + row;
+#pragma unroll
+      for (int r = 0; r < 16; ++r) prefetch_l2(nxt + (size_t)(t + r * TR) * H);
     }
     // the -2 (bit (offset+1) mod q, CUDALucas.cu:1882-1886) hits at most one
     // word; locate it once: element register r_sub, word w_sub

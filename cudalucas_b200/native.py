@@ -23,6 +23,7 @@ LL_ASYNC = 4
 LL_STATIC_MAX_WORDS = 1 << 20
 LL_KERNELS_GENERIC = 1
 LL_KERNELS_NO_FUSED = 2
+LL_KERNELS_NO_PREFETCH = 4
 
 
 class Tuning(ctypes.Structure):

@@ -59,9 +59,11 @@ typedef struct {
 
 /* ll_tuning.kernels: LL_KERNELS_GENERIC forces the generic (runtime-plan)
  * kernels; LL_KERNELS_NO_FUSED keeps short lengths on two launches per
- * iteration instead of the fused cooperative kernel. */
+ * iteration instead of the fused cooperative kernel; LL_KERNELS_NO_PREFETCH
+ * turns off the L2 prefetch that lengths larger than L2 use. */
 #define LL_KERNELS_GENERIC 1
 #define LL_KERNELS_NO_FUSED 2
+#define LL_KERNELS_NO_PREFETCH 4  /* no L2 prefetch of the next wave's data */
 
 /* Creates a context for exponent q at FFT length n (FP64 words) on `device`.
  * Replaces alloc_gpu_mem + write_gpu_data (CUDALucas.cu:1096, :1125).
