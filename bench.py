@@ -442,6 +442,23 @@ def run_batch(args, world, rank, local):
     ms = allreduce_max(t0.elapsed_time(t1), world)
     errs = b.step(1, report=True)
     b.close()
+    other = None
+    if args.batch_compare:
+        # the other launch mode over the same members and steps
+        b2 = cl.LLBatch(qs, ns, device=local, graph_iters=args.batch_graph_iters, by_length=args.batch_per_member)
+        b2.start(offs)
+        for _ in range(W):
+            b2.step(S)
+        b2.sync()
+        ext2 = torch.cuda.ExternalStream(b2.stream, device=torch.device("cuda", local))
+        u0, u1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        u0.record(ext2)
+        for _ in range(K):
+            b2.step(S)
+        u1.record(ext2)
+        b2.sync()
+        b2.close()
+        other = len(members) * K * S * world / (allreduce_max(u0.elapsed_time(u1), world) / 1000.0)
     # the same exponents one at a time, each the same S iterations from the
     # same offset: the serial baseline, and Res64 equal to the batch's
     Ss = args.serial_iters or S
@@ -477,6 +494,7 @@ def run_batch(args, world, rank, local):
                                else "one per pass per member",
                    "serial_iter_s": round(serial_ips, 1), "speedup_vs_serial": round(batch_ips / serial_ips, 3),
                    "serial_sample": "%d iterations of each exponent alone, from the batch's offsets" % Ss,
+                   "other_launch_mode_iter_s": None if other is None else round(other, 1),
                    "max_roundoff_error": round(float(max(errs)), 5)},
         "res64_ok": Ss == S and not mismatched,
         "res64_checked": {"against": "each member run alone for the same %d iterations" % S,
@@ -544,6 +562,8 @@ def main():
     ap.add_argument("--serial-iters", type=int, default=0,
                     help="iterations of each exponent alone in the batch workload's serial leg (0: the step size)")
     ap.add_argument("--serve-hbm-gb", type=float, default=150.0)
+    ap.add_argument("--batch-compare", action="store_true",
+                    help="also time the other launch mode (per member / per length class)")
     ap.add_argument("--batch-per-member", action="store_true",
                     help="launch every member's passes separately instead of once per length class")
     ap.add_argument("--iters-per-step", type=int, default=10000)

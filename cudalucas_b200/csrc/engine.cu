@@ -425,8 +425,8 @@ using L3072 = RList<16, 12, 16>;
 using L3584 = RList<16, 14, 16>;
 using L4096 = RList<16, 16, 16>;
 // column lengths of the tall_any kernels
-using C24 = RList<12, 2>;
-using C28 = RList<14, 2>;
+using C24 = RList<4, 6>;
+using C28 = RList<4, 7>;
 using C100 = RList<10, 10>;
 using C112 = RList<16, 7>;
 using C120 = RList<12, 10>;
@@ -462,24 +462,27 @@ static const StaticWide kWide[] = {
 // Column lengths outside the 16 x M x 16 family that the length policy meets
 // with a specialised row length: the fewest stages of radices <= 16, and the
 // fewest threads per column that keep a stage's butterflies of one thread
-// within 16 elements; about 256 threads per CTA.
+// within 16 elements.  These lengths are short and their passes
+// latency-bound, so a CTA takes one or two column pairs: about 128 CTAs at
+// the row lengths they meet (256 for columns up to 252, 512 above), which
+// spreads the loads over many SMs.
 static const StaticTall kTall[] = {
     LLB_TALL(L256),  LLB_TALL(L512),  LLB_TALL(L768),  LLB_TALL(L1024), LLB_TALL(L1280), LLB_TALL(L1536), LLB_TALL(L1792),
     LLB_TALL(L2048), LLB_TALL(L2304), LLB_TALL(L2560), LLB_TALL(L3072), LLB_TALL(L3584), LLB_TALL(L4096),
-    LLB_TALL_ANY(C24, 2, 64),        LLB_TALL_ANY(C28, 2, 64),
-    LLB_TALL_ANY(C100, 10, 12),      LLB_TALL_ANY(C112, 8, 16),
-    LLB_TALL_ANY(C120, 12, 10),      LLB_TALL_ANY(C140, 14, 9),
-    LLB_TALL_ANY(C160, 16, 8),       LLB_TALL_ANY(C168, 14, 9),
-    LLB_TALL_ANY(C192, 16, 8),       LLB_TALL_ANY(C224, 16, 8),
-    LLB_TALL_ANY(C240, 24, 5),    LLB_TALL_ANY(C252, 28, 4),
-    LLB_TALL_ANY(C288, 32, 4),     LLB_TALL_ANY(C320, 32, 4),
-    LLB_TALL_ANY(C336, 28, 4),    LLB_TALL_ANY(C360, 40, 3),
-    LLB_TALL_ANY(C392, 28, 4),    LLB_TALL_ANY(C400, 40, 3),
-    LLB_TALL_ANY(C448, 32, 4),    LLB_TALL_ANY(C576, 48, 2),
-    LLB_TALL_ANY(C600, 60, 2),    LLB_TALL_ANY(C648, 72, 1),
-    LLB_TALL_ANY(C672, 56, 2),    LLB_TALL_ANY(C720, 72, 1),
-    LLB_TALL_ANY(C784, 56, 2),     LLB_TALL_ANY(C800, 80, 1),
-    LLB_TALL_ANY(C1568, 112, 1),   LLB_TALL_ANY(C2744, 196, 1),
+    LLB_TALL_ANY(C24, 6, 1),        LLB_TALL_ANY(C28, 7, 1),
+    LLB_TALL_ANY(C100, 10, 1),      LLB_TALL_ANY(C112, 8, 1),
+    LLB_TALL_ANY(C120, 12, 1),      LLB_TALL_ANY(C140, 14, 1),
+    LLB_TALL_ANY(C160, 16, 1),      LLB_TALL_ANY(C168, 14, 1),
+    LLB_TALL_ANY(C192, 16, 1),      LLB_TALL_ANY(C224, 16, 1),
+    LLB_TALL_ANY(C240, 24, 1),      LLB_TALL_ANY(C252, 28, 1),
+    LLB_TALL_ANY(C288, 32, 2),      LLB_TALL_ANY(C320, 32, 2),
+    LLB_TALL_ANY(C336, 28, 2),      LLB_TALL_ANY(C360, 40, 2),
+    LLB_TALL_ANY(C392, 28, 2),      LLB_TALL_ANY(C400, 40, 2),
+    LLB_TALL_ANY(C448, 32, 2),      LLB_TALL_ANY(C576, 48, 2),
+    LLB_TALL_ANY(C600, 60, 2),      LLB_TALL_ANY(C648, 72, 2),
+    LLB_TALL_ANY(C672, 56, 2),      LLB_TALL_ANY(C720, 72, 2),
+    LLB_TALL_ANY(C784, 56, 2),      LLB_TALL_ANY(C800, 80, 2),
+    LLB_TALL_ANY(C1568, 112, 1),    LLB_TALL_ANY(C2744, 196, 1),
 };
 
 // Fused cooperative kernels (fused_iters) for short lengths: the shape
@@ -498,10 +501,9 @@ struct FusedKernel {
    std::max(G * row_slots<LW::L, G>() + tw_size<LW>(),                                                     \
             TC ? 2 * PP * col_slots<LT::L>() + tw_size<LT>() : padded(2 * LT::L) + tall_extra<LT>())}
 static const FusedKernel kFused[] = {
-    LLB_FUSED(L256, 4, C24, 2, 16),
-    LLB_FUSED(L256, 4, C28, 2, 16),
+    LLB_FUSED(L256, 4, C24, 6, 8),
+    LLB_FUSED(L256, 4, C28, 7, 16),
     LLB_FUSED(L256, 4, C112, 8, 4),
-    LLB_FUSED(L256, 4, L256, 0, 1),
 };
 static const FusedKernel *find_fused(int W, int H) {
   for (const auto &k : kFused)

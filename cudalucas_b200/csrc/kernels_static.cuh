@@ -228,7 +228,9 @@ constexpr int tall_threads() { return 2 * (P::L / 16); }
 
 // Blocks per SM to ask of the register allocator: about 128 registers per
 // thread, which leaves room for two or more CTAs per SM.
-constexpr int min_blocks(int threads) { return 65536 / (threads * 128) > 1 ? 65536 / (threads * 128) : 1; }
+constexpr int min_blocks(int threads) {
+  return 65536 / (threads * 128) > 32 ? 32 : 65536 / (threads * 128) > 1 ? 65536 / (threads * 128) : 1;
+}
 
 // Shared memory of the tall pass beyond the two columns: stage twiddles,
 // the column twiddle factors w_N^(k*TR*r) of both columns (2 x 16) and the
@@ -885,6 +887,8 @@ template <class PW, int G, class TP>
 __global__ void __launch_bounds__(fused_threads<PW, G, TP>(), 1)
     fused_iters(TallArgs ta, WideArgs wa, uint32_t iters, int tall_units) {
   constexpr int TPB = fused_threads<PW, G, TP>(), T1 = wide_threads<PW, G>(), T2 = TP::threads;
+  static_assert((T1 == TPB || T1 % 32 == 0) && (T2 == TPB || T2 % 32 == 0),
+                "a pass on part of the CTA needs whole warps (named barrier)");
   const int wide_units = wa.ngroups;
   for (uint32_t it = 0; it < iters; ++it) {
     for (int u = blockIdx.x; u < tall_units; u += gridDim.x) {
