@@ -108,7 +108,11 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def dist_init():
+def dist_init(backend="nccl"):
+    """One process per GPU (torchrun's RANK/LOCAL_RANK/WORLD_SIZE); NCCL on
+    GPUs, gloo for the CPU tests of this plumbing.  Every rank runs its own
+    exponent (replicas); the group carries only the max-over-ranks of the
+    timings and the Res64 verdicts."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -116,9 +120,12 @@ def dist_init():
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return world, rank, local
 
 
@@ -127,7 +134,8 @@ def allreduce_max(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
