@@ -292,3 +292,13 @@ def test_cli_long_selftest(cli, tmp_path):
     r = subprocess.run([cli, "-r", "1"], cwd=str(tmp_path), capture_output=True, text=True, timeout=900)
     assert r.returncode == 0, r.stdout[-2000:]
     assert r.stdout.count("This residue is correct.") == 92
+
+
+@pytest.mark.gpu
+def test_cli_polite_mode(cli, tmp_path):
+    """-polite 25 reads the GPU state back every 25 iterations instead of every
+    100 (CUDALucas.cu:1979); the result is unchanged."""
+    (tmp_path / "CUDALucas.ini").write_text(INI)
+    r = run(cli, "-polite", "25", "86243", cwd=str(tmp_path))
+    assert r.returncode == 0, r.stderr
+    assert final_line(tmp_path).startswith("M( 86243 )P, offset = ")
