@@ -62,7 +62,9 @@ def time_shape(q, n, iters, tuning=None, device=0):
     import torch
     ctx = engine.LLContext(q, n, device=device, tuning=tuning)
     ctx.start(0)
-    ctx.step(min(iters, 20))
+    # warm-up long enough to capture the context's CUDA graph (64 iterations)
+    # before the timed region
+    ctx.step(130)
     ctx.sync()
     ext = torch.cuda.ExternalStream(ctx.stream)
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
