@@ -455,7 +455,7 @@ using C1568 = RList<16, 14, 7>;
 using C2744 = RList<14, 14, 14>;
 
 static const StaticWide kWide[] = {
-    LLB_WIDE(L256, 4),  LLB_WIDE(L512, 4),  LLB_WIDE(L768, 4),  LLB_WIDE(L1024, 2), LLB_WIDE(L1280, 2),
+    LLB_WIDE(L256, 4),  LLB_WIDE(L256, 2),  LLB_WIDE(L512, 4),  LLB_WIDE(L768, 4),  LLB_WIDE(L1024, 2), LLB_WIDE(L1280, 2),
     LLB_WIDE(L1536, 2), LLB_WIDE(L1792, 2), LLB_WIDE(L2048, 2), LLB_WIDE(L2304, 2),
     LLB_WIDE(L2560, 2), LLB_WIDE(L3072, 2), LLB_WIDE(L3584, 1), LLB_WIDE(L4096, 1),
 };
@@ -609,6 +609,15 @@ bool shape_ok(long long N, int W, int G, Shape &s) {
 
 // W near sqrt(N); G rows per wide-pass CTA such that a CTA's rows stay
 // within ~100 KB of shared memory (two CTAs per SM).
+// Of two rows-per-CTA counts G for one row length: the larger as long as it
+// leaves at least 32 row groups (CTAs of the wide pass), else the smaller,
+// so that short lengths spread their rows over more SMs.
+static bool prefer_rows(long long H, int g, int cur) {
+  const bool ok_g = H / g >= 32, ok_c = H / cur >= 32;
+  if (ok_g != ok_c) return ok_g;
+  return ok_g ? g > cur : g < cur;
+}
+
 bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
   if (N % 2 || !seven_smooth(N)) return false;
   // compile-time specialised kernels for both passes, W closest to sqrt(N)
@@ -623,7 +632,7 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
       const StaticTall *tt = find_tall((int)H);
       if (!tt || H % w.G) continue;
       const double d = fabs(log((double)w.L / sqrt((double)N)));
-      if (d < best) {
+      if (d < best || (d == best && bw && bw->L == w.L && prefer_rows(H, w.G, bw->G))) {
         best = d;
         bw = &w;
         bt = tt;
@@ -648,7 +657,7 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
       Shape s;
       if (H % w.G || !shape_ok(N, w.L, w.G, s) || s.T2 > TMAX || s.H > EPT * s.T2) continue;
       const double d = fabs(log((double)w.L / sqrt((double)N)));
-      if (d < best) {
+      if (d < best || (d == best && bw && bw->L == w.L && prefer_rows(H, w.G, bw->G))) {
         best = d;
         bw = &w;
         out = s;
@@ -955,9 +964,10 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
         ctx->pdl = ww <= 4 && wt <= 4;
       }
     }
-    // Short lengths with a fused kernel run their plain iterations as one
-    // cooperative launch, when all its CTAs fit on the GPU at once.
-    if (s.sw && s.st && !(tuning && (tuning->kernels & LL_KERNELS_NO_FUSED))) {
+    // On request, short lengths with a fused kernel run their plain
+    // iterations as one cooperative launch, when all its CTAs fit on the GPU
+    // at once.
+    if (s.sw && s.st && tuning && (tuning->kernels & LL_KERNELS_FUSED)) {
       const FusedKernel *f = find_fused(s.W, s.H);
       int sms = 0, per_sm = 0, coop = 0;
       if (f && cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess && coop &&
@@ -1612,7 +1622,7 @@ struct ll_batch {
   cudaStream_t stream = nullptr;
   std::vector<cudaEvent_t> events;  // [0] fork, [1..] joins
   int graph_iters = 0;
-  bool by_class = true;                 // one launch per pass per length class
+  bool by_class = false;                // one launch per pass per length class (else per member)
   std::vector<BatchClass> classes;
   std::vector<int> singles;             // members launched on their own
   cudaGraph_t graph = nullptr;
@@ -1719,7 +1729,6 @@ ll_status ll_batch_create(int device, int32_t count, const uint32_t *q, const ui
   b->graph_iters = graph_iters > 0 ? graph_iters : 10;
   ll_tuning t{};
   t.graph_iters = -1;  // members never capture their own graphs
-  t.kernels = LL_KERNELS_NO_FUSED;  // members run in the batch's graph
   for (int32_t i = 0; i < count; ++i) {
     ll_ctx *c = nullptr;
     ll_status s = ll_create(device, q[i], n[i], &t, &c);

@@ -136,7 +136,7 @@ class LLContext:
 class LLBatch:
     """Many exponents advancing together (ll_batch_* in include/llb200.h)."""
 
-    def __init__(self, qs, ns, device=0, graph_iters=10, by_length=True):
+    def __init__(self, qs, ns, device=0, graph_iters=10, by_length=False):
         L = native.lib()
         self.qs = [int(x) for x in qs]
         self.ns = [int(x) for x in ns]
@@ -148,8 +148,8 @@ class LLBatch:
         if rc:
             raise LLError(rc, "ll_batch_create")
         self._keep = (q, n)
-        if not by_length:
-            L.ll_batch_group_by_length(self._h, 0)
+        if by_length:
+            L.ll_batch_group_by_length(self._h, 1)
 
     @property
     def classes(self):

@@ -22,7 +22,7 @@ LL_ERRCHK = 2
 LL_ASYNC = 4
 LL_STATIC_MAX_WORDS = 1 << 20
 LL_KERNELS_GENERIC = 1
-LL_KERNELS_NO_FUSED = 2
+LL_KERNELS_FUSED = 2
 LL_KERNELS_NO_PREFETCH = 4
 
 

@@ -58,11 +58,14 @@ typedef struct {
 } ll_tuning;
 
 /* ll_tuning.kernels: LL_KERNELS_GENERIC forces the generic (runtime-plan)
- * kernels; LL_KERNELS_NO_FUSED keeps short lengths on two launches per
- * iteration instead of the fused cooperative kernel; LL_KERNELS_NO_PREFETCH
- * turns off the L2 prefetch that lengths larger than L2 use. */
+ * kernels; LL_KERNELS_FUSED runs the plain iterations of the short lengths
+ * that have a fused cooperative kernel (12K, 14K, 56K) as one launch with
+ * grid barriers between the passes, instead of two launches per iteration
+ * (measured slower at 12K and 14K, equal at 56K, so not the default);
+ * LL_KERNELS_NO_PREFETCH turns off the L2 prefetch that lengths larger than
+ * L2 use. */
 #define LL_KERNELS_GENERIC 1
-#define LL_KERNELS_NO_FUSED 2
+#define LL_KERNELS_FUSED 2
 #define LL_KERNELS_NO_PREFETCH 4  /* no L2 prefetch of the next wave's data */
 
 /* Creates a context for exponent q at FFT length n (FP64 words) on `device`.
@@ -164,11 +167,12 @@ ll_status ll_batch_step(ll_batch *b, uint32_t iters, uint32_t flags, float *max_
 ll_status ll_batch_sync(ll_batch *b);
 void *ll_batch_stream(const ll_batch *b);  /* stream the step graphs run on */
 /* Members of one FFT length whose passes have specialised kernels form a
- * length class: by default one launch per pass runs the pass for every
- * member of the class (the graph then has one branch per class, 2 kernel
- * nodes per iteration).  on = 0 launches every member's passes separately
- * (one branch per member); call before the first ll_batch_step.
- * ll_batch_classes gives the number of length classes. */
+ * length class.  on = 1 makes one launch per pass run the pass for every
+ * member of the class (the step graph then has one branch per class, 2
+ * kernel nodes per iteration); the default, on = 0, launches every member's
+ * passes separately (one branch per member), which measured about 5 %
+ * faster on the 256-exponent benchmark set.  Call before the first
+ * ll_batch_step.  ll_batch_classes gives the number of length classes. */
 ll_status ll_batch_group_by_length(ll_batch *b, int32_t on);
 int32_t ll_batch_classes(const ll_batch *b);
 ll_status ll_batch_res64(ll_batch *b, uint64_t *res64);

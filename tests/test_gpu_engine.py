@@ -275,13 +275,14 @@ def test_specialised_columns_of_any_radix_list(nk):
 
 @pytest.mark.parametrize("n", [12288, 14336, 57344])
 def test_fused_iterations_equal_two_launch_iterations(n):
-    """Short lengths run their plain iterations as one cooperative launch
-    with grid barriers between the passes; the digits are bit for bit those
-    of two launches per iteration, and match the oracle's residue."""
+    """On request, short lengths run their plain iterations as one
+    cooperative launch with grid barriers between the passes; the digits are
+    bit for bit those of two launches per iteration, and match the oracle's
+    residue."""
     q = _exponent_at(n)
     off = q // 3
-    d1, o1, e1, s1 = engine_run(q, n, off, 700)
-    d2, o2, e2, s2 = engine_run(q, n, off, 700, kernels=cl.native.LL_KERNELS_NO_FUSED)
+    d1, o1, e1, s1 = engine_run(q, n, off, 700, kernels=cl.native.LL_KERNELS_FUSED)
+    d2, o2, e2, s2 = engine_run(q, n, off, 700)
     assert s1["fused"] and not s2["fused"], (s1, s2)
     assert o1 == o2 and np.array_equal(d1, d2) and e1 == e2
     o = Oracle(q, n)
