@@ -276,15 +276,19 @@ def test_specialised_columns_of_any_radix_list(nk):
 @pytest.mark.parametrize("n", [12288, 14336, 57344])
 def test_fused_iterations_equal_two_launch_iterations(n):
     """On request, short lengths run their plain iterations as one
-    cooperative launch with grid barriers between the passes; the digits are
-    bit for bit those of two launches per iteration, and match the oracle's
-    residue."""
+    cooperative launch with grid barriers between the passes; the value (the
+    digits modulo 2^q-1) equals that of two launches per iteration and the
+    oracle's residue.  The fused kernel hands carries between groups of 4
+    rows while the two-launch path uses groups of 2 for short rows, so the
+    balanced digits themselves differ in representation."""
     q = _exponent_at(n)
     off = q // 3
     d1, o1, e1, s1 = engine_run(q, n, off, 700, kernels=cl.native.LL_KERNELS_FUSED)
     d2, o2, e2, s2 = engine_run(q, n, off, 700)
     assert s1["fused"] and not s2["fused"], (s1, s2)
-    assert o1 == o2 and np.array_equal(d1, d2) and e1 == e2
+    assert o1 == o2
+    assert np.array_equal(cl.standardize(d1, q, n)[0], cl.standardize(d2, q, n)[0])
+    assert e1 < 0.4 and e2 < 0.4 and e1 <= 2 * e2 + 1e-3 and e2 <= 2 * e1 + 1e-3, (e1, e2)
     o = Oracle(q, n)
     o.start(off)
     o.step(700)
