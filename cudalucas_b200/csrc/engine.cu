@@ -33,6 +33,7 @@
 // pass runs in a few waves: the next kernel's CTAs load their constant tables
 // while the previous pass drains, and wait (griddepcontrol.wait) before they
 // touch the state.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stddef.h>
@@ -44,6 +45,7 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/llb200.h"
@@ -373,6 +375,7 @@ __global__ void __launch_bounds__(256) wide_kernel(WideArgs a) {
 }
 
 #include "kernels_static.cuh"
+#include "kernels_cluster.cuh"
 
 // Registry of compile-time specialised kernels, by row length.
 struct StaticWide {
@@ -401,7 +404,9 @@ struct StaticTall {
    wide_static_batch<LIST, G>,                                                                                  \
    LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tw_size<LIST>(),             \
    G * row_slots<LIST::L, G>()}
-#define LLB_RAD(LIST) LIST::N, {LIST::a[0], LIST::N > 1 ? LIST::a[1 % LIST::N] : 0, LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}
+#define LLB_RAD(LIST)                                                                                 \
+  LIST::N, {LIST::a[0], LIST::N > 1 ? LIST::a[1 % LIST::N] : 0, LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, \
+            LIST::N > 3 ? LIST::a[3 % LIST::N] : 0}
 #define LLB_TALL(LIST) \
   {LIST::L, tall_static<LIST>, tall_static_batch<LIST>, LLB_RAD(LIST), tw_size<LIST>(),                      \
    padded(2 * LIST::L) + tall_extra<LIST>(), 2 * (LIST::L / 16), 1}
@@ -489,27 +494,51 @@ static const StaticTall kTall[] = {
 // (row length W, column length H) they are compiled for.  The tall pass uses
 // fewer column pairs per CTA than the two-launch kernels, for more CTAs.
 struct FusedKernel {
-  int W, H;
+  int W, H, G;  // G: rows per wide-pass unit (must equal the context's)
   void (*run)(TallArgs, WideArgs, uint32_t, int);
   int threads;      // per CTA
   int tall_ppc;     // column pairs per tall unit
   int smem;         // dynamic shared-memory entries
 };
 #define LLB_FUSED(LW, G, LT, TC, PP)                                                                        \
-  {LW::L, LT::L, fused_iters<LW, G, FusedTall<LT, TC, PP>>, fused_threads<LW, G, FusedTall<LT, TC, PP>>(), \
+  {LW::L, LT::L, G, fused_iters<LW, G, FusedTall<LT, TC, PP>>, fused_threads<LW, G, FusedTall<LT, TC, PP>>(), \
    TC ? PP : 1,                                                                                              \
    std::max(G * row_slots<LW::L, G>() + tw_size<LW>(),                                                     \
             TC ? 2 * PP * col_slots<LT::L>() + tw_size<LT>() : padded(2 * LT::L) + tall_extra<LT>())}
 static const FusedKernel kFused[] = {
-    LLB_FUSED(L256, 4, C24, 6, 8),
-    LLB_FUSED(L256, 4, C28, 7, 16),
-    LLB_FUSED(L256, 4, C112, 8, 4),
+    LLB_FUSED(L256, 2, C24, 6, 8),
+    LLB_FUSED(L256, 2, C28, 7, 16),
+    LLB_FUSED(L256, 2, C112, 8, 4),
 };
-static const FusedKernel *find_fused(int W, int H) {
+static const FusedKernel *find_fused(int W, int H, int G) {
   for (const auto &k : kFused)
-    if (k.W == W && k.H == H) return &k;
+    if (k.W == W && k.H == H && k.G == G) return &k;
   return nullptr;
 }
+
+// Cluster-resident kernels (cluster_iters) for short lengths: the shape
+// (W, H), the row radix list and threads per row, the cluster size C and
+// the launch.  Of the entries of a shape, the first whose cluster can be
+// scheduled on the device is used (ll_tuning.cluster_variant picks another).
+struct ClusterKernel {
+  int W, H, C;
+  void (*run)(TallArgs, WideArgs, const double2 *, uint32_t, int);
+  int nrad, rad[4];  // row radix list
+  int tw;            // its stage twiddle entries
+  int threads;       // per CTA
+  int smem;          // dynamic shared-memory entries
+};
+#define LLB_CLUSTER(PR, TWR, LT, TC, C, RPC)                                                                     \
+  {PR::L, LT::L, C, cluster_iters<PR, TWR, LT, TC, C, RPC>, LLB_RAD(PR), tw_size<PR>(),                         \
+   ClusterCfg<PR, TWR, LT, TC, C, RPC>::T, ClusterCfg<PR, TWR, LT, TC, C, RPC>::total}
+using R256A = RList<4, 4, 4, 4>;  // 64 threads per row, one radix-4 butterfly each per stage
+using R256B = RList<8, 4, 8>;     // 32 threads per row
+static const ClusterKernel kCluster[] = {
+    LLB_CLUSTER(R256A, 64, C24, 6, 16, 2),    LLB_CLUSTER(R256B, 32, C24, 6, 16, 2),
+    LLB_CLUSTER(R256A, 64, C24, 6, 8, 4),     LLB_CLUSTER(R256B, 32, C28, 7, 16, 2),
+    LLB_CLUSTER(R256A, 64, C28, 7, 8, 4),     LLB_CLUSTER(R256A, 64, C100, 10, 16, 10),
+    LLB_CLUSTER(R256A, 64, C112, 8, 16, 8),   LLB_CLUSTER(R256A, 64, C192, 16, 16, 12),
+};
 
 static const StaticTall *find_tall(int L) {
   for (const auto &k : kTall)
@@ -759,6 +788,8 @@ struct ll_ctx {
   bool pdl = false;  // chain the passes with programmatic dependent launch
   const FusedKernel *fused = nullptr;  // iterations as one cooperative launch
   int fused_grid = 0;
+  const ClusterKernel *cluster = nullptr;  // iterations as one cluster-resident launch
+  double2 *stwC = nullptr;                 // stage twiddles of its row radix list
   float pending_err = 0.f;
   std::string err;
   TallArgs ta{};
@@ -794,7 +825,7 @@ static void free_ctx(ll_ctx *c) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(c->device);
-  void *ptrs[] = {c->A, c->xint, c->ck_digits, c->carry, c->flags, c->st, c->twW, c->twH, c->thi, c->tlo, c->stwW, c->stwH,
+  void *ptrs[] = {c->A, c->xint, c->ck_digits, c->carry, c->flags, c->st, c->twW, c->twH, c->thi, c->tlo, c->stwW, c->stwH, c->stwC,
                   c->rowE, c->colF, c->rowW, c->rowWi, c->colW, c->colWi};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -968,7 +999,7 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
     // iterations as one cooperative launch, when all its CTAs fit on the GPU
     // at once.
     if (s.sw && s.st && tuning && (tuning->kernels & LL_KERNELS_FUSED)) {
-      const FusedKernel *f = find_fused(s.W, s.H);
+      const FusedKernel *f = find_fused(s.W, s.H, s.G);
       int sms = 0, per_sm = 0, coop = 0;
       if (f && cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess && coop &&
           cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
@@ -981,6 +1012,50 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
           ctx->fused = f;
           ctx->fused_grid = units;
         }
+      }
+    }
+    // Short lengths with a cluster-resident kernel run every step as one
+    // launch of one thread-block cluster (the default; LL_KERNELS_CLUSTER8
+    // keeps to clusters of at most 8 CTAs, LL_KERNELS_NO_CLUSTER turns it off).
+    if (s.sw && s.st && !ctx->fused && !(tuning && (tuning->kernels & LL_KERNELS_NO_CLUSTER))) {
+      int cl_ok = 0;
+      if (cudaDeviceGetAttribute(&cl_ok, cudaDevAttrClusterLaunch, device) != cudaSuccess) cl_ok = 0;
+      int variant = 0;
+      for (const auto &k : kCluster) {
+        if (!cl_ok || k.W != s.W || k.H != s.H) continue;
+        if (k.C > 8 && tuning && (tuning->kernels & LL_KERNELS_CLUSTER8)) continue;
+        if (tuning && tuning->cluster_variant > 0 && variant++ != tuning->cluster_variant) continue;
+        const size_t bytes = sizeof(double2) * (size_t)k.smem;
+        if (cudaFuncSetAttribute(k.run, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess ||
+            (k.C > 8 && cudaFuncSetAttribute(k.run, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
+          cudaGetLastError();
+          continue;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)k.C);
+        cfg.blockDim = dim3((unsigned)k.threads);
+        cfg.dynamicSmemBytes = bytes;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)k.C;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)k.run, &cfg) != cudaSuccess) {
+          cudaGetLastError();
+          continue;
+        }
+        if (nclusters > 0) {
+          ctx->cluster = &k;
+          break;
+        }
+      }
+      if (ctx->cluster) {
+        std::vector<double2> t = stage_twiddles(ctx->cluster->rad, ctx->cluster->nrad);
+        if ((int)t.size() != ctx->cluster->tw) { rc = LL_ERR_SHAPE; break; }
+        if ((e = upload(&ctx->stwC, t)) != cudaSuccess) { rc = cuda_fail(ctx, e, "upload"); break; }
       }
     }
     TallArgs &ta = ctx->ta;
@@ -1142,6 +1217,35 @@ static ll_status launch_fused(ll_ctx *ctx, uint32_t iters) {
   return LL_OK;
 }
 
+// Iterations as cluster-resident launches (at most 65536 per launch, a
+// fraction of a second at the lengths that have such a kernel); the last
+// launch writes the digits when the step reports.
+static ll_status launch_cluster(ll_ctx *ctx, uint32_t iters, bool report) {
+  const ClusterKernel *f = ctx->cluster;
+  for (uint32_t done = 0; done < iters;) {
+    uint32_t k = std::min<uint32_t>(iters - done, 65536u);
+    int rep = report && done + k == iters ? 1 : 0;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)f->C);
+    cfg.blockDim = dim3((unsigned)f->threads);
+    cfg.dynamicSmemBytes = sizeof(double2) * (size_t)f->smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)f->C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const double2 *stw = ctx->stwC;
+    void *argv[] = {(void *)&ctx->ta, (void *)&ctx->wa, (void *)&stw, (void *)&k, (void *)&rep};
+    CK(cudaLaunchKernelExC(&cfg, (const void *)f->run, argv));
+    for (uint32_t i = 0; i < k; ++i) ctx->offset = (uint32_t)((2ull * ctx->offset) % ctx->q);
+    done += k;
+  }
+  return LL_OK;
+}
+
 ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
   if (!ctx) return LL_ERR_ARG;
   if (!ctx->started) return LL_ERR_STATE;
@@ -1154,7 +1258,11 @@ ll_status ll_step(ll_ctx *ctx, uint32_t iters, uint32_t flags, float *max_err) {
   const bool report = (flags & LL_REPORT) != 0;
   uint32_t done = 0;
   const uint32_t K = (uint32_t)ctx->graph_iters;
-  if (ctx->fused && iters >= 2u + (report ? 1u : 0u)) {
+  if (ctx->cluster && iters) {
+    const ll_status rc = launch_cluster(ctx, iters, report);
+    if (rc != LL_OK) return rc;
+    done = iters;
+  } else if (ctx->fused && iters >= 2u + (report ? 1u : 0u)) {
     // plain iterations fused; the report iteration (if any) as two passes
     const uint32_t plain = iters - (report ? 1u : 0u);
     const ll_status rc = launch_fused(ctx, plain);
@@ -1311,9 +1419,23 @@ void ll_shape(const ll_ctx *ctx, int32_t *width, int32_t *height, int32_t *rows_
   if (threads_tall) *threads_tall = ctx->shape.T2;
 }
 const char *ll_last_error(const ll_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+int32_t ll_check_tables(void) {
+  int32_t bad = 0;
+  for (const auto &k : kWide)
+    if ((int)stage_twiddles(k.rad, k.nrad).size() != k.extra) ++bad;
+  for (const auto &k : kTall)
+    if ((int)stage_twiddles(k.rad, k.nrad).size() != k.tw) ++bad;
+  for (const auto &k : kCluster) {
+    int L = 1;
+    for (int i = 0; i < k.nrad; ++i) L *= k.rad[i];
+    if (L != k.W || (int)stage_twiddles(k.rad, k.nrad).size() != k.tw) ++bad;
+  }
+  return bad;
+}
+
 int32_t ll_kernel_kinds(const ll_ctx *ctx) {
   if (!ctx) return 0;
-  return (ctx->shape.sw ? 1 : 0) | (ctx->shape.st ? 2 : 0) | (ctx->fused ? 4 : 0);
+  return (ctx->shape.sw ? 1 : 0) | (ctx->shape.st ? 2 : 0) | (ctx->fused ? 4 : 0) | (ctx->cluster ? 8 : 0);
 }
 void ll_debug_inject_failure(ll_ctx *ctx, int32_t count) {
   if (ctx) ctx->inject = count;

@@ -130,6 +130,7 @@ class LLContext:
         d = dict(zip(("W", "H", "G", "threads_wide", "threads_tall"), [x.value for x in v]))
         k = native.lib().ll_kernel_kinds(self._h)
         d["wide_specialised"], d["tall_specialised"], d["fused"] = bool(k & 1), bool(k & 2), bool(k & 4)
+        d["cluster"] = bool(k & 8)
         return d
 
 

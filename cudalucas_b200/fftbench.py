@@ -6,7 +6,10 @@ G) of each length is timed with CUDA events on the context's stream, and the
 fastest is printed (and optionally written as a tuning table).
 
   python -m cudalucas_b200.fftbench 3200K [18432K ...] [--iters 200]
-         [--width W] [--rows G] [--all-shapes] [--table FILE]
+         [--width W] [--rows G] [--kernels FLAGS] [--all-shapes] [--table FILE]
+
+--kernels passes ll_tuning.kernels (LL_KERNELS_* flags, e.g. 8 = no
+cluster-resident iterations).
 """
 import argparse
 import ctypes
@@ -112,6 +115,8 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=200)
     ap.add_argument("--width", type=int, default=0)
     ap.add_argument("--rows", type=int, default=0)
+    ap.add_argument("--kernels", type=int, default=0)
+    ap.add_argument("--variant", type=int, default=0, help="cluster kernel variant (ll_tuning.cluster_variant)")
     ap.add_argument("--all-shapes", action="store_true")
     ap.add_argument("--table", default="")
     ap.add_argument("--device", type=int, default=0)
@@ -128,12 +133,17 @@ def main(argv=None):
                 t["width"] = args.width
             if args.rows:
                 t["rows_per_cta"] = args.rows
+            if args.kernels:
+                t["kernels"] = args.kernels
+            if args.variant:
+                t["cluster_variant"] = args.variant
             shapes = [t or None]
         best = None
         for t in shapes:
             ms, tall, wide, err, shape = time_shape(q, n, args.iters, t, args.device)
-            print("%8dK q=%d W=%d H=%d G=%d  %.4f ms/iter  tall %.1f us  wide %.1f us  err %.5f"
-                  % (n // 1024, q, shape["W"], shape["H"], shape["G"], ms, tall, wide, err), flush=True)
+            print("%8dK q=%d W=%d H=%d G=%d%s  %.4f ms/iter  tall %.1f us  wide %.1f us  err %.5f"
+                  % (n // 1024, q, shape["W"], shape["H"], shape["G"], " cluster" if shape.get("cluster") else "",
+                     ms, tall, wide, err), flush=True)
             if best is None or ms < best[0]:
                 best = (ms, shape)
         table[n] = {"ms_per_iter": best[0], **best[1]}

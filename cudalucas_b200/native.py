@@ -24,13 +24,15 @@ LL_STATIC_MAX_WORDS = 1 << 20
 LL_KERNELS_GENERIC = 1
 LL_KERNELS_FUSED = 2
 LL_KERNELS_NO_PREFETCH = 4
+LL_KERNELS_NO_CLUSTER = 8
+LL_KERNELS_CLUSTER8 = 16
 
 
 class Tuning(ctypes.Structure):
     _fields_ = [("width", ctypes.c_int32), ("rows_per_cta", ctypes.c_int32),
                 ("threads_wide", ctypes.c_int32), ("threads_tall", ctypes.c_int32),
                 ("graph_iters", ctypes.c_int32), ("kernels", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 2)]
+                ("cluster_variant", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 _lib = None
@@ -67,6 +69,7 @@ def lib():
         "ll_shape": (None, [vp, i32p, i32p, i32p, i32p, i32p]),
         "ll_last_error": (ctypes.c_char_p, [vp]),
         "ll_kernel_kinds": (i32, [vp]),
+        "ll_check_tables": (i32, []),
         "ll_status_string": (ctypes.c_char_p, [i32]),
         "ll_debug_inject_failure": (None, [vp, i32]),
         "ll_debug_launch": (i32, [vp, i32]),

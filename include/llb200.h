@@ -54,7 +54,10 @@ typedef struct {
   int32_t threads_tall; /* threads per CTA of the tall pass                 */
   int32_t graph_iters;  /* iterations captured per CUDA graph (0 = auto)    */
   int32_t kernels;      /* LL_KERNELS_* flags (0 = the engine's choice)     */
-  int32_t reserved[2];
+  int32_t cluster_variant; /* among the cluster-resident kernels of the
+                              length: 0 = the first that fits the device,
+                              v > 0 = the v-th entry (0-based)               */
+  int32_t reserved;
 } ll_tuning;
 
 /* ll_tuning.kernels: LL_KERNELS_GENERIC forces the generic (runtime-plan)
@@ -63,10 +66,16 @@ typedef struct {
  * grid barriers between the passes, instead of two launches per iteration
  * (measured slower at 12K and 14K, equal at 56K, so not the default);
  * LL_KERNELS_NO_PREFETCH turns off the L2 prefetch that lengths larger than
- * L2 use. */
+ * L2 use.  Short lengths with a cluster-resident kernel (12K, 14K, 50K, 56K,
+ * 96K) run each ll_step as one launch of one thread-block cluster whose
+ * shared memory holds the whole state; LL_KERNELS_NO_CLUSTER turns that off
+ * (two launches per iteration), LL_KERNELS_CLUSTER8 keeps to the portable
+ * cluster size of 8 CTAs. */
 #define LL_KERNELS_GENERIC 1
 #define LL_KERNELS_FUSED 2
 #define LL_KERNELS_NO_PREFETCH 4  /* no L2 prefetch of the next wave's data */
+#define LL_KERNELS_NO_CLUSTER 8   /* no cluster-resident iterations */
+#define LL_KERNELS_CLUSTER8 16    /* clusters of at most 8 CTAs */
 
 /* Creates a context for exponent q at FFT length n (FP64 words) on `device`.
  * Replaces alloc_gpu_mem + write_gpu_data (CUDALucas.cu:1096, :1125).
@@ -134,8 +143,15 @@ void ll_shape(const ll_ctx *ctx, int32_t *width, int32_t *height,
 const char *ll_last_error(const ll_ctx *ctx); /* text of the last failure   */
 /* Which passes run compile-time specialised kernels: bit 0 the wide (row)
  * pass, bit 1 the tall (column) pass (the others use the generic kernels);
- * bit 2: plain iterations run as fused cooperative launches. */
+ * bit 2: plain iterations run as fused cooperative launches; bit 3: every
+ * step runs as cluster-resident launches (the state in the shared memory of
+ * one thread-block cluster). */
 int32_t ll_kernel_kinds(const ll_ctx *ctx);
+/* Host-only self-check of the compiled kernel tables: the number of
+ * specialised kernels whose stage-twiddle table (built on the host from the
+ * recorded radix list) does not have the size the kernel reads.  0 when
+ * consistent; needs no GPU. */
+int32_t ll_check_tables(void);
 const char *ll_status_string(ll_status s);
 
 /* Test hook (CUDALucas.cu:2938-2950 handles a CUDA error from lucas_square

@@ -163,3 +163,10 @@ def test_fft_max_exponent_inverts_the_lower_bound():
     for n in (12288, 3276800, 18874368):
         q = cl.fft_max_exponent(n)
         assert cl.fft_bounds(q)[0] <= n < cl.fft_bounds(q + 1)[0]
+
+
+def test_kernel_tables_are_consistent():
+    """Every specialised kernel's stage-twiddle table, built on the host from
+    the radix list recorded beside it, has the size the kernel reads (the
+    cluster kernels' row lists of four radices included)."""
+    assert native.lib().ll_check_tables() == 0

@@ -276,20 +276,54 @@ def test_specialised_columns_of_any_radix_list(nk):
 @pytest.mark.parametrize("n", [12288, 14336, 57344])
 def test_fused_iterations_equal_two_launch_iterations(n):
     """On request, short lengths run their plain iterations as one
-    cooperative launch with grid barriers between the passes; the value (the
-    digits modulo 2^q-1) equals that of two launches per iteration and the
-    oracle's residue.  The fused kernel hands carries between groups of 4
-    rows while the two-launch path uses groups of 2 for short rows, so the
-    balanced digits themselves differ in representation."""
+    cooperative launch with grid barriers between the passes.  The carry of
+    element (m1, m2) comes from element (m1, m2-1) whichever CTA holds it, so
+    the digits are bit for bit those of two launches per iteration; they
+    match the oracle's residue."""
     q = _exponent_at(n)
     off = q // 3
     d1, o1, e1, s1 = engine_run(q, n, off, 700, kernels=cl.native.LL_KERNELS_FUSED)
-    d2, o2, e2, s2 = engine_run(q, n, off, 700)
-    assert s1["fused"] and not s2["fused"], (s1, s2)
-    assert o1 == o2
-    assert np.array_equal(cl.standardize(d1, q, n)[0], cl.standardize(d2, q, n)[0])
-    assert e1 < 0.4 and e2 < 0.4 and e1 <= 2 * e2 + 1e-3 and e2 <= 2 * e1 + 1e-3, (e1, e2)
+    d2, o2, e2, s2 = engine_run(q, n, off, 700, kernels=cl.native.LL_KERNELS_NO_CLUSTER)
+    assert s1["fused"] and not s2["fused"] and not s2["cluster"], (s1, s2)
+    assert o1 == o2 and np.array_equal(d1, d2) and e1 == e2
     o = Oracle(q, n)
     o.start(off)
     o.step(700)
     assert cl.digits_res64(d1, q, n, o1) == o.res64()
+
+
+@pytest.mark.parametrize("n", [12288, 14336, 51200, 57344, 98304])
+def test_cluster_iterations_equal_two_launch_iterations(n):
+    """Short lengths run every step as one launch of one thread-block
+    cluster whose shared memory holds the state (cluster_iters).  After many
+    iterations (several launches, a report in the last one) the digits are
+    bit for bit those of two launches per iteration (the rounded values
+    agree), the roundoff maximum agrees within rounding (the row transforms
+    are factored differently), and the residue is the oracle's."""
+    q = _exponent_at(n)
+    off = q // 3
+    with cl.LLContext(q, n) as c:
+        assert c.shape["cluster"], c.shape
+        c.start(off)
+        e1 = max(c.step(333, report=True), c.step(1, report=True), c.step(366, report=True))
+        d1, o1 = c.read_digits()
+    d2, o2, e2, s2 = engine_run(q, n, off, 700, kernels=cl.native.LL_KERNELS_NO_CLUSTER)
+    assert not s2["cluster"]
+    assert o1 == o2 and np.array_equal(d1, d2), (o1, o2)
+    assert e1 < 0.4 and e1 <= 1.5 * e2 + 1e-3 and e2 <= 1.5 * e1 + 1e-3, (e1, e2)
+    o = Oracle(q, n)
+    o.start(off)
+    o.step(700)
+    assert cl.digits_res64(d1, q, n, o1) == o.res64()
+
+
+@pytest.mark.parametrize("tuning", [{"kernels": 16}, {"cluster_variant": 1}, {"cluster_variant": 2}])
+def test_cluster_variants_agree(tuning):
+    """The cluster variants of 12K (clusters of 16 or 8 CTAs, rows on 64 or
+    32 threads) give the same digits as the default and the exact residue."""
+    q, n = 216091, 12288
+    d1, o1, e1, s1 = engine_run(q, n, 77, 500, **tuning)
+    d0, o0, e0, s0 = engine_run(q, n, 77, 500)
+    assert s1["cluster"] and s0["cluster"]
+    assert o1 == o0 and np.array_equal(d1, d0)
+    assert cl.digits_res64(d1, q, n, o1) == exact.res64(q, 500)
