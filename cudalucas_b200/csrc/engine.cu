@@ -413,8 +413,7 @@ struct StaticTall {
 // any radix list: TC threads per column, PP column pairs per CTA
 #define LLB_TALL_ANY(LIST, TC, PP)                                                                       \
   {LIST::L, tall_any<LIST, TC, PP>, tall_any_batch<LIST, TC, PP>, LLB_RAD(LIST), tw_size<LIST>(),          \
-   2 * PP * col_slots<LIST::L>() + tw_size<LIST>(),                                                           \
-   2 * PP * TC, PP}
+   tall_any_smem<LIST, PP>(), 2 * PP * TC, PP}
 
 using L256 = RList<16, 16>;
 using L512 = RList<16, 2, 16>;
@@ -504,7 +503,7 @@ struct FusedKernel {
   {LW::L, LT::L, G, fused_iters<LW, G, FusedTall<LT, TC, PP>>, fused_threads<LW, G, FusedTall<LT, TC, PP>>(), \
    TC ? PP : 1,                                                                                              \
    std::max(G * row_slots<LW::L, G>() + tw_size<LW>(),                                                     \
-            TC ? 2 * PP * col_slots<LT::L>() + tw_size<LT>() : padded(2 * LT::L) + tall_extra<LT>())}
+            TC ? tall_any_smem<LT, PP>() : padded(2 * LT::L) + tall_extra<LT>())}
 static const FusedKernel kFused[] = {
     LLB_FUSED(L256, 2, C24, 6, 8),
     LLB_FUSED(L256, 2, C28, 7, 16),
@@ -523,21 +522,34 @@ static const FusedKernel *find_fused(int W, int H, int G) {
 struct ClusterKernel {
   int W, H, C;
   void (*run)(TallArgs, WideArgs, const double2 *, uint32_t, int);
-  int nrad, rad[4];  // row radix list
-  int tw;            // its stage twiddle entries
-  int threads;       // per CTA
-  int smem;          // dynamic shared-memory entries
+  int nrad, rad[4];    // row radix list
+  int ncrad, crad[4];  // column radix list
+  int tw;              // stage twiddle entries of both lists
+  int threads;         // per CTA
+  int smem;            // dynamic shared-memory entries
 };
+#define LLB_CRAD(LIST)                                                                                \
+  LIST::N, {LIST::a[0], LIST::N > 1 ? LIST::a[1 % LIST::N] : 0, LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, \
+            LIST::N > 3 ? LIST::a[3 % LIST::N] : 0}
 #define LLB_CLUSTER(PR, TWR, LT, TC, C, RPC)                                                                     \
-  {PR::L, LT::L, C, cluster_iters<PR, TWR, LT, TC, C, RPC>, LLB_RAD(PR), tw_size<PR>(),                         \
+  {PR::L, LT::L, C, cluster_iters<PR, TWR, LT, TC, C, RPC>, LLB_RAD(PR), LLB_CRAD(LT), tw_size<PR>() + tw_size<LT>(), \
    ClusterCfg<PR, TWR, LT, TC, C, RPC>::T, ClusterCfg<PR, TWR, LT, TC, C, RPC>::total}
-using R256A = RList<4, 4, 4, 4>;  // 64 threads per row, one radix-4 butterfly each per stage
-using R256B = RList<8, 4, 8>;     // 32 threads per row
+// row lists of 256: 64 threads per row (one radix-4 butterfly each per
+// stage) or 32 threads per row
+using R256A = RList<4, 4, 4, 4>;
+using R256B = RList<8, 4, 8>;
+// column lists of small radices: many threads per column, short chains
+using K24 = RList<4, 6>;
+using K28 = RList<4, 7>;
+using K112 = RList<4, 4, 7>;
+// Only lengths where one cluster (16 SMs) beats two launches over the whole
+// GPU: at 12K 4.9 vs 10.0 us/iter, 14K 5.7 vs 10.0, 56K 13.3 vs 18.6; at
+// 50K (15.7 vs 12.8) and 96K (21.7 vs 16.7) the arithmetic of 16 SMs is the
+// bound and the two-launch path stays.
 static const ClusterKernel kCluster[] = {
-    LLB_CLUSTER(R256A, 64, C24, 6, 16, 2),    LLB_CLUSTER(R256B, 32, C24, 6, 16, 2),
-    LLB_CLUSTER(R256A, 64, C24, 6, 8, 4),     LLB_CLUSTER(R256B, 32, C28, 7, 16, 2),
-    LLB_CLUSTER(R256A, 64, C28, 7, 8, 4),     LLB_CLUSTER(R256A, 64, C100, 10, 16, 10),
-    LLB_CLUSTER(R256A, 64, C112, 8, 16, 8),   LLB_CLUSTER(R256A, 64, C192, 16, 16, 12),
+    LLB_CLUSTER(R256A, 64, K24, 6, 16, 2),    LLB_CLUSTER(R256B, 32, K24, 6, 16, 2),
+    LLB_CLUSTER(R256A, 64, K24, 6, 8, 4),     LLB_CLUSTER(R256B, 32, K28, 7, 16, 2),
+    LLB_CLUSTER(R256A, 64, K28, 7, 8, 4),     LLB_CLUSTER(R256B, 32, K112, 28, 16, 8),
 };
 
 static const StaticTall *find_tall(int L) {
@@ -1054,6 +1066,8 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
       }
       if (ctx->cluster) {
         std::vector<double2> t = stage_twiddles(ctx->cluster->rad, ctx->cluster->nrad);
+        const std::vector<double2> tc = stage_twiddles(ctx->cluster->crad, ctx->cluster->ncrad);
+        t.insert(t.end(), tc.begin(), tc.end());
         if ((int)t.size() != ctx->cluster->tw) { rc = LL_ERR_SHAPE; break; }
         if ((e = upload(&ctx->stwC, t)) != cudaSuccess) { rc = cuda_fail(ctx, e, "upload"); break; }
       }
@@ -1426,9 +1440,12 @@ int32_t ll_check_tables(void) {
   for (const auto &k : kTall)
     if ((int)stage_twiddles(k.rad, k.nrad).size() != k.tw) ++bad;
   for (const auto &k : kCluster) {
-    int L = 1;
+    int L = 1, Lc = 1;
     for (int i = 0; i < k.nrad; ++i) L *= k.rad[i];
-    if (L != k.W || (int)stage_twiddles(k.rad, k.nrad).size() != k.tw) ++bad;
+    for (int i = 0; i < k.ncrad; ++i) Lc *= k.crad[i];
+    if (L != k.W || Lc != k.H ||
+        (int)(stage_twiddles(k.rad, k.nrad).size() + stage_twiddles(k.crad, k.ncrad).size()) != k.tw)
+      ++bad;
   }
   return bad;
 }

@@ -49,71 +49,6 @@
 // while the roundoff error stays below 0.5); the roundoff maximum differs in
 // its last bits, the row transforms being factored differently.
 
-// One Stockham stage of one row with TR threads, like sstage, but the
-// elements are read through ld(e) and the outputs written through st(e, v)
-// (e: index within the row).  INPLACE: the stage reads and writes the same
-// slots, so a barrier separates the loads from the stores.
-template <int L, int R, int NS, int SIGN, int TR, bool INPLACE, class S, class LD, class ST>
-__device__ __forceinline__ void fstage(const double2 *tw, int t, S sync, LD ld, ST st) {
-  constexpr int M = L / R;
-  constexpr int NB = (M + TR - 1) / TR;
-  constexpr bool kShared = NS > 1 && NB > 1 && TR % NS == 0 && R <= 8;
-  double2 wk[kShared ? R - 1 : 1];
-  if constexpr (kShared) {
-#pragma unroll
-    for (int r = 1; r < R; ++r) wk[r - 1] = tw[(int)((unsigned)t % NS) * tw_stride(R) + r - 1];
-  }
-  double2 v[NB][R];
-#pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    const int j = t + b * TR;
-    if (M % TR == 0 || j < M) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) v[b][r] = ld(j + r * M);
-      if constexpr (NS > 1) {
-        const int k = (int)((unsigned)j % NS);
-#pragma unroll
-        for (int r = 1; r < R; ++r) {
-          const double2 w = kShared ? wk[r - 1] : tw[k * tw_stride(R) + r - 1];
-          v[b][r] = SIGN > 0 ? cmul(v[b][r], w) : cmulc(v[b][r], w);
-        }
-      }
-      sdft<R, SIGN>(v[b]);
-    }
-  }
-  if constexpr (INPLACE && !(NB == 1 && NS == M)) sync();
-#pragma unroll
-  for (int b = 0; b < NB; ++b) {
-    const int j = t + b * TR;
-    if (M % TR == 0 || j < M) {
-      const int k = (int)((unsigned)j % NS);
-      const int ob = (j - k) * R + k;
-#pragma unroll
-      for (int r = 0; r < R; ++r) st(ob + r * NS, v[b][sslot<R>(r)]);
-    }
-  }
-  sync();
-}
-
-// All stages of the radix list P: the first reads through ld0, the last
-// writes through stN (both in place when they are the plain ld/st), the
-// others read and write the row in place through ld/st.
-// The last stage stores elsewhere (another CTA, registers): no barrier
-// between its loads and stores; its closing barrier still orders its loads
-// before later writes to the row.
-template <class P, int I, int NS, int TR, int SIGN, class S, class LD0, class STN, class LD, class ST>
-__device__ __forceinline__ void fall_stages(const double2 *tw, int t, S sync, LD0 ld0, STN stN, LD ld, ST st) {
-  static_assert(P::N >= 2, "first and last stage distinct");
-  if constexpr (I < P::N) {
-    constexpr int R = P::a[I];
-    const double2 *tws = tw + tw_offset<P, I>();
-    if constexpr (I == 0) fstage<P::L, R, NS, SIGN, TR, true>(tws, t, sync, ld0, st);
-    else if constexpr (I == P::N - 1) fstage<P::L, R, NS, SIGN, TR, false>(tws, t, sync, ld, stN);
-    else fstage<P::L, R, NS, SIGN, TR, true>(tws, t, sync, ld, st);
-    fall_stages<P, I + 1, NS * R, TR, SIGN>(tw, t, sync, ld0, stN, ld, st);
-  }
-}
-
 template <class PR, int TWR, class PT, int TC, int C, int RPC>
 struct ClusterCfg {
   static constexpr int W = PR::L, H = PT::L;
@@ -175,6 +110,7 @@ __device__ __forceinline__ double2 *cluster_slot(cooperative_groups::cluster_gro
 template <class PR, int TWR, class PT, int TC, int C, int RPC>
 __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
     cluster_iters(TallArgs ta, WideArgs wa, const double2 *stwr, uint32_t iters, int report) {
+  // stwr: stage twiddles of the row list PR, then of the column list PT
   using CF = ClusterCfg<PR, TWR, PT, TC, C, RPC>;
   constexpr int W = CF::W, H = CF::H, EPR = CF::EPR, PPC = CF::PPC, CS = CF::CS, RS = CF::RS, PS = CF::PS;
   constexpr int T = CF::T, TT = CF::TT, TW = CF::TW;
@@ -195,7 +131,7 @@ __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
   // ---- set-up: tables, twiddles of the owned columns, the owned state
   if (tid == 0) s_fault = 0;
   for (int i = tid; i < tw_size<PR>(); i += T) stw[i] = stwr[i];
-  for (int i = tid; i < tw_size<PT>(); i += T) stt[i] = ta.stw[i];
+  for (int i = tid; i < tw_size<PT>(); i += T) stt[i] = stwr[tw_size<PR>() + i];
   for (int i = tid; i < W; i += T) {
     cwt[i] = make_double2(wa.colW[i], wa.colWi[i]);
     cf[i] = wa.colF[i];
@@ -264,10 +200,10 @@ __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
     if (tid < TT) {
       double2 *cc = cols + col * CS;
       const double2 *cw = ctw + col * H;
-      auto ld = [&](int e) { return cc[pad(e)]; };
-      auto st = [&](int e, double2 v) { cc[pad(e)] = v; };
-      auto ld_tw = [&](int e) { return cmul(cc[pad(e)], cw[e]); };
-      fall_stages<PT, 0, 1, TC, +1>(stt, tc, syncT, ld_tw, st, ld, st);
+      auto ld = [&](int e, int, int) { return cc[pad(e)]; };
+      auto st = [&](int e, int, int, double2 v) { cc[pad(e)] = v; };
+      auto ld_tw = [&](int e, int, int) { return cmul(cc[pad(e)], cw[e]); };
+      fall_stages<PT, 0, 1, TC, +1, true, true>(stt, tc, syncT, ld_tw, st, ld, st);
       const int ti = tid - 2 * pl * TC;
       double2 *ra = cols + 2 * pl * CS, *rb = ra + CS;
       const double2 *pw = ptw + pl * PS;
@@ -296,10 +232,10 @@ __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
       syncT();
       // the last inverse stage: conjugate twiddle, then element (my_k1, e)
       // into the row buffer of the CTA that owns row e
-      auto st_push = [&](int e, double2 v) {
+      auto st_push = [&](int e, int, int, double2 v) {
         *cl.map_shared_rank(rows + (e % RPC) * RS + pad(my_k1), (unsigned)(e / RPC)) = cmulc(v, cw[e]);
       };
-      fall_stages<PT, 0, 1, TC, -1>(stt, tc, syncT, ld, st_push, ld, st);
+      fall_stages<PT, 0, 1, TC, -1, true, false>(stt, tc, syncT, ld, st_push, ld, st);
     }
     cl.sync();  // every row buffer holds its row
     // ---------------------------------------------------------- wide pass
@@ -318,10 +254,10 @@ __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
       const bool w_sub = dw & 1;
       // inverse row transform; its last stage leaves elements t + j*TWR in u[j]
       double2 u[EPR];
-      auto ld = [&](int e) { return rw[pad(e)]; };
-      auto st = [&](int e, double2 v) { rw[pad(e)] = v; };
-      auto st_reg = [&](int e, double2 v) { u[(e - t) / TWR] = v; };
-      fall_stages<PR, 0, 1, TWR, -1>(stw, t, syncW, ld, st_reg, ld, st);
+      auto ld = [&](int e, int, int) { return rw[pad(e)]; };
+      auto st = [&](int e, int, int, double2 v) { rw[pad(e)] = v; };
+      auto st_reg = [&](int, int, int r, double2 v) { u[r] = v; };
+      fall_stages<PR, 0, 1, TWR, -1, true, false>(stw, t, syncW, ld, st_reg, ld, st);
 #pragma unroll
       for (int j = 0; j < EPR; ++j) {
         const int m1 = t + j * TWR;
@@ -386,11 +322,11 @@ __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
       // forward row transform: the first stage takes x[j] from registers
       // (its barrier orders the carry reads above before the row is
       // rewritten); the last stores element (k1, m2) into its column owner
-      auto ld = [&](int e) { return rw[pad(e)]; };
-      auto st = [&](int e, double2 v) { rw[pad(e)] = v; };
-      auto ld_reg = [&](int e) { return x[(e - t) / TWR]; };
-      auto st_push = [&](int e, double2 v) { *cluster_slot<CF>(cl, cols, e, m2) = v; };
-      fall_stages<PR, 0, 1, TWR, +1>(stw, t, syncW, ld_reg, st_push, ld, st);
+      auto ld = [&](int e, int, int) { return rw[pad(e)]; };
+      auto st = [&](int e, int, int, double2 v) { rw[pad(e)] = v; };
+      auto ld_reg = [&](int, int, int r) { return x[r]; };
+      auto st_push = [&](int e, int, int, double2 v) { *cluster_slot<CF>(cl, cols, e, m2) = v; };
+      fall_stages<PR, 0, 1, TWR, +1, true, false>(stw, t, syncW, ld_reg, st_push, ld, st);
     }
     cl.sync();  // the state is whole again
   }

@@ -454,6 +454,77 @@ __device__ __forceinline__ void all_stages(double2 *s, const double2 *tw, int ro
   }
 }
 
+// One Stockham stage of one row with TR threads, like sstage, but the
+// elements are read through ld(e, j, r) and the outputs written through
+// st(e, j, r, v): e is the index within the row, j the butterfly and r the
+// element of the butterfly (loads: e = j + r*L/R; stores of the last stage,
+// where NS = L/R: e = j + r*NS).  INPLACE: the stage reads and writes the same
+// slots, so a barrier separates the loads from the stores.
+template <int L, int R, int NS, int SIGN, int TR, bool INPLACE, class S, class LD, class ST>
+__device__ __forceinline__ void fstage(const double2 *tw, int t, S sync, LD ld, ST st) {
+  constexpr int M = L / R;
+  constexpr int NB = (M + TR - 1) / TR;
+  constexpr bool kShared = NS > 1 && NB > 1 && TR % NS == 0 && R <= 8;
+  double2 wk[kShared ? R - 1 : 1];
+  if constexpr (kShared) {
+#pragma unroll
+    for (int r = 1; r < R; ++r) wk[r - 1] = tw[(int)((unsigned)t % NS) * tw_stride(R) + r - 1];
+  }
+  double2 v[NB][R];
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const int j = t + b * TR;
+    if (M % TR == 0 || j < M) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = ld(j + r * M, j, r);
+      if constexpr (NS > 1) {
+        const int k = (int)((unsigned)j % NS);
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const double2 w = kShared ? wk[r - 1] : tw[k * tw_stride(R) + r - 1];
+          v[b][r] = SIGN > 0 ? cmul(v[b][r], w) : cmulc(v[b][r], w);
+        }
+      }
+      sdft<R, SIGN>(v[b]);
+    }
+  }
+  if constexpr (INPLACE && !(NB == 1 && NS == M)) sync();
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
+    const int j = t + b * TR;
+    if (M % TR == 0 || j < M) {
+      const int k = (int)((unsigned)j % NS);
+      const int ob = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) st(ob + r * NS, j, r, v[b][sslot<R>(r)]);
+    }
+  }
+  sync();
+}
+
+// All stages of the radix list P: the first reads through ld0, the last
+// writes through stN (both in place when they are the plain ld/st), the
+// others read and write the row in place through ld/st.
+// FIRSTIN: the first stage's loads read the row (or must be ordered before
+// its stores into the row, e.g. reads of other slots by other threads): a
+// barrier between its loads and stores.  LASTIN: the last stage stores into
+// the row it reads; otherwise it stores elsewhere (global memory, another
+// CTA, registers) and its closing barrier still orders its loads before
+// later writes to the row.
+template <class P, int I, int NS, int TR, int SIGN, bool FIRSTIN, bool LASTIN, class S, class LD0, class STN, class LD,
+          class ST>
+__device__ __forceinline__ void fall_stages(const double2 *tw, int t, S sync, LD0 ld0, STN stN, LD ld, ST st) {
+  static_assert(P::N >= 2, "first and last stage distinct");
+  if constexpr (I < P::N) {
+    constexpr int R = P::a[I];
+    const double2 *tws = tw + tw_offset<P, I>();
+    if constexpr (I == 0) fstage<P::L, R, NS, SIGN, TR, FIRSTIN>(tws, t, sync, ld0, st);
+    else if constexpr (I == P::N - 1) fstage<P::L, R, NS, SIGN, TR, LASTIN>(tws, t, sync, ld, stN);
+    else fstage<P::L, R, NS, SIGN, TR, true>(tws, t, sync, ld, st);
+    fall_stages<P, I + 1, NS * R, TR, SIGN, FIRSTIN, LASTIN>(tw, t, sync, ld0, stN, ld, st);
+  }
+}
+
 // Tall pass for column lengths H = P::L outside the 16 x M x 16 family (any
 // radix list of 2..16): PP column pairs per CTA, TC threads per column, every
 // stage in shared memory.  A column is loaded with the twiddle w_N^(k1*m2)
@@ -462,11 +533,22 @@ __device__ __forceinline__ void all_stages(double2 *s, const double2 *tw, int ro
 // with conjugate twiddles and stored with the conjugate twiddle.  The same
 // arithmetic as the generic tall kernel, with every index and loop bound a
 // constant.
+// Shared memory of a tall_any CTA (double2 entries): 2*PP padded columns,
+// the stage twiddles, and per column the factors w_N^(k1*M0*r) of the first
+// stage's loads (r < a[0], M0 = H/a[0]) and w_N^(k1*NS*r) of the last
+// stage's stores (r < a[N-1], NS = H/a[N-1]).
+template <class P, int PP>
+__host__ __device__ constexpr int tall_any_smem() {
+  return 2 * PP * col_slots<P::L>() + tw_size<P>() + 2 * PP * (P::a[0] + P::a[P::N - 1]);
+}
+
 template <class P, int TC, int PP, class S = CtaSync>
 __device__ __forceinline__ void tall_any_body(const TallArgs &a, int blk, S sync = S()) {
   constexpr int H = P::L, CS = col_slots<H>(), T = 2 * PP * TC;
+  constexpr int R0 = P::a[0], RN = P::a[P::N - 1], M0 = H / R0, NSN = H / RN, FS = R0 + RN;
   extern __shared__ double2 sm[];
   double2 *stw = sm + 2 * PP * CS;
+  double2 *fac = stw + tw_size<P>();
   const int units = a.W / 2;
   const int col = threadIdx.x / TC, t = threadIdx.x - col * TC;  // col < 2*PP
   const int pl = col >> 1;
@@ -475,8 +557,16 @@ __device__ __forceinline__ void tall_any_body(const TallArgs &a, int blk, S sync
   const bool special = c == 0;
   const int W = a.W;
   const int kA = special ? 0 : c, kB = special ? W / 2 : W - c;
-  const int k1 = (col & 1) ? kB : kA;
+  // column of this thread (column 0 for the threads of a pair past the last
+  // one: they read valid memory and store nothing)
+  const int k1 = !active ? 0 : (col & 1) ? kB : kA;
   for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
+  for (int i = threadIdx.x; i < 2 * PP * FS; i += T) {
+    const int cc = i / FS, r = i - cc * FS;
+    const int cp = blk * PP + (cc >> 1);
+    const int kk = cp >= units ? 0 : (cc & 1) ? (cp == 0 ? W / 2 : W - cp) : cp;
+    fac[i] = omegaN(a.thi, a.tlo, a.ts, a.tmask, r < R0 ? kk * M0 * r : kk * NSN * (r - R0));
+  }
   griddep_wait();
   griddep_release();
   if (blk == 0 && threadIdx.x == 0) {
@@ -484,20 +574,30 @@ __device__ __forceinline__ void tall_any_body(const TallArgs &a, int blk, S sync
     a.st->offset = (uint32_t)((2ull * o) % a.q);
   }
   double2 *row = sm + col * CS;
-  if (active) {
-    const double2 *src = a.A + (size_t)k1 * H;
-    for (int m2 = t; m2 < H; m2 += TC) row[pad(m2)] = cmul(src[m2], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
-  }
+  const double2 *fc = fac + col * FS;
+  double2 *gcol = a.A + (size_t)k1 * H;
   cp_async_wait_all();
   sync();
-  all_stages<P, CS, 0, 1, TC, +1>(sm, stw, col, t, sync);
+  // the column twiddle w_N^(k1*m2) of element m2 = j + r*X (a butterfly j of
+  // the first or last stage) is w_N^(k1*j) (once per butterfly) times the
+  // stage's factor r of this column
+  double2 base = make_double2(1.0, 0.0);
+  auto ld = [&](int e, int, int) { return row[pad(e)]; };
+  auto st = [&](int e, int, int, double2 v) { row[pad(e)] = v; };
+  auto ld_first = [&](int e, int j, int r) {
+    if (r == 0) base = omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * j);
+    return active ? cmul(gcol[e], r == 0 ? base : cmul(base, fc[r])) : make_double2(0.0, 0.0);
+  };
+  fall_stages<P, 0, 1, TC, +1, false, true>(stw, t, sync, ld_first, st, ld, st);
   if (active) {
     const int ti = threadIdx.x - 2 * pl * TC;  // thread of the pair, < 2*TC
     double2 *ra = sm + 2 * pl * CS, *rb = ra + CS;
+    // pairing twiddle w_N^(kb + W*k2) = w_N^kb * w_H^k2
     if (!special) {
+      const double2 wb = omegaN(a.thi, a.tlo, a.ts, a.tmask, kA);
       for (int k2 = ti; k2 < H; k2 += 2 * TC) {  // bin k2 of column kA <-> bin H-1-k2 of column kB
         double2 za = ra[pad(k2)], zb = rb[pad(H - 1 - k2)];
-        pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, kA + W * k2));
+        pair_square(za, zb, cmul(wb, __ldg(&a.twH[k2])));
         ra[pad(k2)] = za;
         rb[pad(H - 1 - k2)] = zb;
       }
@@ -505,24 +605,25 @@ __device__ __forceinline__ void tall_any_body(const TallArgs &a, int blk, S sync
       for (int i = ti; i <= H / 2; i += 2 * TC) {  // column 0: k2 <-> (H-k2) mod H
         const int p2 = (H - i) % H;
         double2 za = ra[pad(i)], zb = ra[pad(p2)];
-        pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W * i));
+        pair_square(za, zb, __ldg(&a.twH[i]));
         ra[pad(i)] = za;
         if (p2 != i) ra[pad(p2)] = zb;
       }
+      const double2 wb = omegaN(a.thi, a.tlo, a.ts, a.tmask, W / 2);
       for (int i = ti; i < H / 2; i += 2 * TC) {  // column W/2: k2 <-> H-1-k2
         double2 za = rb[pad(i)], zb = rb[pad(H - 1 - i)];
-        pair_square(za, zb, omegaN(a.thi, a.tlo, a.ts, a.tmask, W / 2 + W * i));
+        pair_square(za, zb, cmul(wb, __ldg(&a.twH[i])));
         rb[pad(i)] = za;
         rb[pad(H - 1 - i)] = zb;
       }
     }
   }
   sync();
-  all_stages<P, CS, 0, 1, TC, -1>(sm, stw, col, t, sync);
-  if (active) {
-    double2 *dst = a.A + (size_t)k1 * H;
-    for (int m2 = t; m2 < H; m2 += TC) dst[m2] = cmulc(row[pad(m2)], omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * m2));
-  }
+  auto st_last = [&](int e, int j, int r, double2 v) {
+    if (r == 0) base = omegaN(a.thi, a.tlo, a.ts, a.tmask, k1 * j);
+    if (active) gcol[e] = cmulc(v, r == 0 ? base : cmul(base, fc[R0 + r]));
+  };
+  fall_stages<P, 0, 1, TC, -1, true, false>(stw, t, sync, ld, st_last, ld, st);
 }
 
 template <class P, int TC, int PP>
