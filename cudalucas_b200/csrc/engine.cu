@@ -539,17 +539,28 @@ struct ClusterKernel {
 using R256A = RList<4, 4, 4, 4>;
 using R256B = RList<8, 4, 8>;
 // column lists of small radices: many threads per column, short chains
+using K16 = RList<4, 4>;
+using K20 = RList<4, 5>;
 using K24 = RList<4, 6>;
 using K28 = RList<4, 7>;
+using K32 = RList<4, 8>;
+using K36 = RList<6, 6>;
+using K40 = RList<5, 8>;
+using K64 = RList<4, 4, 4>;
 using K112 = RList<4, 4, 7>;
 // Only lengths where one cluster (16 SMs) beats two launches over the whole
-// GPU: at 12K 4.9 vs 10.0 us/iter, 14K 5.7 vs 10.0, 56K 13.3 vs 18.6; at
-// 50K (15.7 vs 12.8) and 96K (21.7 vs 16.7) the arithmetic of 16 SMs is the
-// bound and the two-launch path stays.
+// GPU (us per iteration, cluster against two launches): 8K 3.6 / 13.4, 10K
+// 5.1 / 15.6, 12K 4.8 / 9.9, 14K 5.7 / 10.0, 16K 4.8 / 17.2, 18K 6.1 / 17.7,
+// 20K 6.5 / 16.3, 32K 7.8 / 16.5, 56K 13.1 / 14.8.  At 50K (15.7 / 11.7) and
+// 96K (21.7 / 12.1) the arithmetic of 16 SMs is the bound and the two-launch
+// path stays.  The entries cover shapes with rows of 256 only.
 static const ClusterKernel kCluster[] = {
+    LLB_CLUSTER(R256A, 64, K16, 4, 16, 1),    LLB_CLUSTER(R256B, 32, K20, 5, 16, 2),
     LLB_CLUSTER(R256A, 64, K24, 6, 16, 2),    LLB_CLUSTER(R256B, 32, K24, 6, 16, 2),
     LLB_CLUSTER(R256A, 64, K24, 6, 8, 4),     LLB_CLUSTER(R256B, 32, K28, 7, 16, 2),
-    LLB_CLUSTER(R256A, 64, K28, 7, 8, 4),     LLB_CLUSTER(R256B, 32, K112, 28, 16, 8),
+    LLB_CLUSTER(R256A, 64, K28, 7, 8, 4),     LLB_CLUSTER(R256A, 64, K32, 8, 16, 2),
+    LLB_CLUSTER(R256B, 32, K36, 6, 16, 3),    LLB_CLUSTER(R256A, 64, K40, 8, 16, 4),
+    LLB_CLUSTER(R256A, 64, K64, 16, 16, 4),   LLB_CLUSTER(R256B, 32, K112, 28, 16, 8),
 };
 
 static const StaticTall *find_tall(int L) {
@@ -1029,7 +1040,10 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
     // Short lengths with a cluster-resident kernel run every step as one
     // launch of one thread-block cluster (the default; LL_KERNELS_CLUSTER8
     // keeps to clusters of at most 8 CTAs, LL_KERNELS_NO_CLUSTER turns it off).
-    if (s.sw && s.st && !ctx->fused && !(tuning && (tuning->kernels & LL_KERNELS_NO_CLUSTER))) {
+    // (Not when the tuning asks for the generic kernels or their launch shape.)
+    const bool want_generic = tuning && (tuning->rows_per_cta > 0 || tuning->threads_wide > 0 ||
+                                         tuning->threads_tall > 0 || (tuning->kernels & LL_KERNELS_GENERIC));
+    if (!ctx->fused && !want_generic && !(tuning && (tuning->kernels & LL_KERNELS_NO_CLUSTER))) {
       int cl_ok = 0;
       if (cudaDeviceGetAttribute(&cl_ok, cudaDevAttrClusterLaunch, device) != cudaSuccess) cl_ok = 0;
       int variant = 0;

@@ -66,8 +66,8 @@ typedef struct {
  * grid barriers between the passes, instead of two launches per iteration
  * (measured slower at 12K and 14K, equal at 56K, so not the default);
  * LL_KERNELS_NO_PREFETCH turns off the L2 prefetch that lengths larger than
- * L2 use.  Short lengths with a cluster-resident kernel (12K, 14K, 56K) run
- * each ll_step as one launch of one thread-block cluster whose
+ * L2 use.  Short lengths with a cluster-resident kernel (8K, 10K, 12K, 14K,
+ * 16K, 18K, 20K, 32K, 56K) run each ll_step as one launch of one thread-block cluster whose
  * shared memory holds the whole state; LL_KERNELS_NO_CLUSTER turns that off
  * (two launches per iteration), LL_KERNELS_CLUSTER8 keeps to the portable
  * cluster size of 8 CTAs. */
