@@ -387,6 +387,8 @@ struct StaticWide {
   int nrad, rad[4];
   int extra;  // shared-memory entries beyond the rows (stage twiddles)
   int rows;   // shared-memory entries of the G rows
+  int tr;     // threads per row (a thread's elements are t + r*tr)
+  int alt;    // 1: the alternative row kernel of its length (LL_KERNELS_ALT_WIDE)
 };
 struct StaticTall {
   int L;
@@ -403,7 +405,15 @@ struct StaticTall {
   {LIST::L, G, wide_static<LIST, G, WIDE_ITER>, wide_static<LIST, G, WIDE_REPORT>, wide_static<LIST, G, WIDE_INIT>, \
    wide_static_batch<LIST, G>,                                                                                  \
    LIST::N, {LIST::a[0], LIST::a[1], LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, 0}, tw_size<LIST>(),             \
-   G * row_slots<LIST::L, G>()}
+   G * row_slots<LIST::L, G>(), LIST::L / 16, 0}
+// rows through shared memory with few elements per thread (wide_any); MINB
+// CTAs per SM asked of the register allocator
+#define LLB_WIDE_ANY(LIST, G, MINB)                                                                         \
+  {LIST::L, G, wide_any<LIST, G, MINB, WIDE_ITER>, wide_any<LIST, G, MINB, WIDE_REPORT>,                     \
+   wide_any<LIST, G, MINB, WIDE_INIT>, wide_any_batch<LIST, G, MINB>,                                        \
+   LIST::N, {LIST::a[0], LIST::N > 1 ? LIST::a[1 % LIST::N] : 0, LIST::N > 2 ? LIST::a[2 % LIST::N] : 0,       \
+             LIST::N > 3 ? LIST::a[3 % LIST::N] : 0},                                                          \
+   tw_size<LIST>(), G * row_slots<LIST::L, G>(), LIST::L / LIST::a[0], 1}
 #define LLB_RAD(LIST)                                                                                 \
   LIST::N, {LIST::a[0], LIST::N > 1 ? LIST::a[1 % LIST::N] : 0, LIST::N > 2 ? LIST::a[2 % LIST::N] : 0, \
             LIST::N > 3 ? LIST::a[3 % LIST::N] : 0}
@@ -458,11 +468,29 @@ using C800 = RList<16, 10, 5>;
 using C1568 = RList<16, 14, 7>;
 using C2744 = RList<14, 14, 14>;
 
+// Alternative row kernels (opt-in, LL_KERNELS_ALT_WIDE): twice the warps per
+// SM (64-80 registers, 3 CTAs of 8 or 10 warps) but every stage through
+// shared memory.  Measured (ms/iter, alternative against default): 2048K
+// 0.0435 / 0.0366, 3200K 0.0679 / 0.0629, 3136K 0.0643 / 0.0650, 1440K
+// 0.0382 / 0.0418.
+using A1280 = RList<8, 4, 5, 8>;  // 160 threads per row, 8 elements each
+using A1024 = RList<8, 4, 4, 8>;
 static const StaticWide kWide[] = {
     LLB_WIDE(L256, 4),  LLB_WIDE(L256, 2),  LLB_WIDE(L512, 4),  LLB_WIDE(L768, 4),  LLB_WIDE(L1024, 2), LLB_WIDE(L1280, 2),
     LLB_WIDE(L1536, 2), LLB_WIDE(L1792, 2), LLB_WIDE(L2048, 2), LLB_WIDE(L2304, 2),
     LLB_WIDE(L2560, 2), LLB_WIDE(L3072, 2), LLB_WIDE(L3584, 1), LLB_WIDE(L4096, 1),
+    LLB_WIDE_ANY(A1280, 2, 3), LLB_WIDE_ANY(A1024, 2, 3),
 };
+// the row kernel variants a context may use: with LL_KERNELS_ALT_WIDE the
+// alternative kernel of a length replaces the others of that length
+static bool wide_allowed(const StaticWide &w, const ll_tuning *t) {
+  const bool want_alt = t && (t->kernels & LL_KERNELS_ALT_WIDE);
+  if (w.alt) return want_alt;
+  if (!want_alt) return true;
+  for (const auto &k : kWide)
+    if (k.alt && k.L == w.L) return false;
+  return true;
+}
 // Column lengths outside the 16 x M x 16 family that the length policy meets
 // with a specialised row length: the fewest stages of radices <= 16, and the
 // fewest threads per column that keep a stage's butterflies of one thread
@@ -678,7 +706,7 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
     const StaticTall *bt = nullptr;
     double best = 1e30;
     for (const auto &w : kWide) {
-      if (N % w.L) continue;
+      if (N % w.L || !wide_allowed(w, t)) continue;
       if (t && t->width > 0 && t->width != w.L) continue;
       const long long H = N / w.L;
       const StaticTall *tt = find_tall((int)H);
@@ -694,7 +722,7 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
       out.W = bw->L;
       out.H = (int)(N / bw->L);
       out.G = bw->G;
-      out.T1 = bw->G * (bw->L / 16);
+      out.T1 = bw->G * bw->tr;
       out.T2 = bt->threads;
       out.sw = bw;
       out.st = bt;
@@ -703,7 +731,7 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
     // a specialised wide pass with the generic tall pass, when the columns
     // have no specialised length (the wide pass is the costlier one)
     for (const auto &w : kWide) {
-      if (N % w.L) continue;
+      if (N % w.L || !wide_allowed(w, t)) continue;
       if (t && t->width > 0 && t->width != w.L) continue;
       const long long H = N / w.L;
       Shape s;
@@ -716,7 +744,7 @@ bool choose_shape(long long N, const ll_tuning *t, Shape &out) {
       }
     }
     if (bw) {
-      out.T1 = bw->G * (bw->L / 16);
+      out.T1 = bw->G * bw->tr;
       out.sw = bw;
       out.st = nullptr;
       return true;
@@ -1112,7 +1140,7 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
     }
     if (s.sw) {
       // column m1 = t + r*TR: exponent colF[t] - D_r (mod n), D_r = r*TR*2H*b mod n
-      const long long TR = s.W / 16;
+      const long long TR = s.sw->tr;
       for (int r = 0; r < 16; ++r) {
         const long long D = (long long)((unsigned __int128)r * TR * 2 * s.H % n * ctx->b % n);
         wa.colD[r] = (int)D;
@@ -1692,7 +1720,7 @@ extern "C" ll_status ll_step_static(int device, uint32_t q, uint32_t n, uint32_t
   wa.st = dst; wa.pw = pw; wa.W = W; wa.H = H; wa.G = s.G; wa.ngroups = ngroups;
   wa.q = q; wa.n = n; wa.b = b; wa.qn = qn;
   if (s.sw) {
-    const long long TR = W / 16;
+    const long long TR = s.sw->tr;
     for (int r = 0; r < 16; ++r) {
       const long long D = (long long)((unsigned __int128)r * TR * 2 * H % n * b % n);
       wa.colD[r] = (int)D;

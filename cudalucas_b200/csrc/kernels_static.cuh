@@ -883,6 +883,209 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   wide_body<P, G, MODE, false>(a, 0);
 }
 
+// Wide pass for rows of length W = P::L whose radix list starts and ends with
+// the same radix R (e.g. 1280 = 8 x 4 x 5 x 8): TR = W/R threads per row, R
+// elements each, every stage in shared memory (Stockham, natural order in and
+// out, the same list both ways).  The first inverse stage reads straight from
+// global memory and the last forward stage writes straight to it; the last
+// inverse butterfly of thread t yields elements t + r*TR, which are what it
+// rounds and carries and what its first forward butterfly takes, so they stay
+// in registers in between.  Fewer elements per thread than wide_body's 16
+// keep the registers per thread low and the warps per SM high.  The carry
+// arithmetic, the -2 and the warp-by-warp hand-off are those of wide_body
+// (colD/colS of the arguments are computed for this TR).
+template <class P, int G, int MODE, bool BATCH, class S = CtaSync>
+__device__ __forceinline__ void wide_any_body(const WideArgs &a, int blk, S sync = S()) {
+  constexpr int W = P::L, R = P::a[0], TR = W / R, T = G * TR;
+  static_assert(P::a[P::N - 1] == R, "first and last radix equal: the carried elements stay in registers");
+  static_assert(G >= 2, "the rows of an element column in adjacent lanes: whole 32-byte sectors");
+  extern __shared__ double2 sm[];
+  constexpr int RS = row_slots<W, G>();
+  double2 *stw = sm + G * RS;
+  __shared__ int s_g;
+  __shared__ float s_err[32];
+  __shared__ uint32_t s_fault;
+  if (threadIdx.x == 0) {
+    s_fault = 0;
+    s_g = MODE == WIDE_INIT ? (BATCH ? blk : (int)blockIdx.x)
+                            : (int)(atomicAdd(&a.st->ticket, 1ull) % (unsigned long long)a.ngroups);
+  }
+  for (int i = threadIdx.x; i < tw_size<P>(); i += T) cp_async16(&stw[i], &a.stw[i]);
+  sync();
+  const int g = s_g;
+  const int H = a.H;
+  const int m2b = g * G;
+  const int row = threadIdx.x % G, t = threadIdx.x / G;
+  const int m2 = m2b + row;
+  const int n = (int)a.n, bb = (int)a.b, qn = (int)a.qn;
+  int E0 = __ldg(&a.rowE[2 * m2]) + __ldg(&a.colF[t]);
+  int E1 = __ldg(&a.rowE[2 * m2 + 1]) + __ldg(&a.colF[t]);
+  const double cwt = __ldg(&a.colW[t]);
+  const double W0 = __ldg(&a.rowW[2 * m2]) * cwt * (E0 >= n ? 0.5 : 1.0);
+  const double W1 = __ldg(&a.rowW[2 * m2 + 1]) * cwt * (E1 >= n ? 0.5 : 1.0);
+  double Wi0 = 0.0, Wi1 = 0.0;
+  if (MODE != WIDE_INIT) {
+    const double cwit = __ldg(&a.colWi[t]);
+    Wi0 = __ldg(&a.rowWi[2 * m2]) * cwit * (E0 >= n ? 2.0 : 1.0);
+    Wi1 = __ldg(&a.rowWi[2 * m2 + 1]) * cwit * (E1 >= n ? 2.0 : 1.0);
+  }
+  if (E0 >= n) E0 -= n;
+  if (E1 >= n) E1 -= n;
+  const double p2lo = (double)(1 << qn), p2hi = 2.0 * p2lo;
+  const double ip2lo = 1.0 / p2lo, ip2hi = 0.5 * ip2lo;
+  double2 *rw = sm + row * RS;
+  auto ld = [&](int e, int, int) { return rw[pad(e)]; };
+  auto st = [&](int e, int, int, double2 v) { rw[pad(e)] = v; };
+  double2 x[R];
+  double emax = 0.0;
+  bool out_of_range = false;
+  // everything above reads constant tables only; the state array, the
+  // digits and the device state are read after the previous pass completed
+  griddep_wait();
+  griddep_release();
+  if (MODE != WIDE_INIT) {
+    // the -2 (bit (offset+1) mod q, CUDALucas.cu:1882-1886) hits at most one
+    // word; locate it once: element register r_sub, word w_sub
+    const uint32_t off = a.st->offset;
+    const uint32_t pos = (off + 1) % a.q;
+    const uint32_t dw = (uint32_t)(((unsigned long long)pos * a.n) / a.q);
+    const uint32_t sdw = (uint32_t)(((unsigned long long)dw * a.q + a.n - 1) / a.n);
+    const double sub = (double)(1u << (pos - sdw));
+    int r_sub = -1;
+    {
+      const uint32_t me = dw >> 1, mm1 = me / (uint32_t)H, mm2 = me - mm1 * (uint32_t)H;
+      if ((int)mm2 == m2 && (int)(mm1 % TR) == t) r_sub = (int)(mm1 / TR);
+    }
+    const bool w_sub = dw & 1;
+    // inverse row transform: the first stage straight from global memory,
+    // the last into registers (elements t + r*TR)
+    const double2 *src = a.A + m2;
+    double2 u[R];
+    auto ld_first = [&](int e, int, int) { return src[(size_t)e * H]; };
+    auto st_reg = [&](int, int, int r, double2 v) { u[r] = v; };
+    cp_async_wait_all();  // the stage twiddles, visible after the first stage's barrier
+    fall_stages<P, 0, 1, TR, -1, false, false>(stw, t, sync, ld_first, st_reg, ld, st);
+    double2 *ks = rw + t;  // ks[r*TR]: element m1 = t + r*TR
+    double *gcd = reinterpret_cast<double *>(a.carry);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int m1 = t + r * TR;
+      const int D = a.colD[r];
+      const bool n0 = E0 < D, n1 = E1 < D;
+      const int e0 = E0 - D + (n0 ? n : 0), e1 = E1 - D + (n1 ? n : 0);
+      const double t0 = u[r].x * (Wi0 * (n0 ? a.colSi2[r] : a.colSi[r]));
+      const double t1 = u[r].y * (Wi1 * (n1 ? a.colSi2[r] : a.colSi[r]));
+      double r0 = rint(t0), r1 = rint(t1);
+      emax = fmax(emax, fmax(fabs(t0 - r0), fabs(t1 - r1)));
+      if (!(fabs(t0) < 0x1p51 && fabs(t1) < 0x1p51)) out_of_range = true;
+      if (r == r_sub) {
+        if (w_sub) r1 -= sub;
+        else r0 -= sub;
+      }
+      const bool big0 = e0 < bb, big1 = e1 < bb;
+      const double P0 = big0 ? p2hi : p2lo, I0 = big0 ? ip2hi : ip2lo;
+      const double P1 = big1 ? p2hi : p2lo, I1 = big1 ? ip2hi : ip2lo;
+      const double h0 = rnd_int(r0 * I0), l0 = fma(-h0, P0, r0);
+      const double h1 = rnd_int(r1 * I1), l1 = fma(-h1, P1, r1);
+      const double tt1 = l1 + h0;
+      const double k1c = rnd_int(tt1 * I1);
+      const double d1p = fma(-k1c, P1, tt1);
+      const double co = h1 + k1c;
+      ks[r * TR] = make_double2(fma(d1p, 0x1p24, l0), co);
+      if (row == G - 1) gcd[(size_t)g * W + m1] = co;
+    }
+    // hand-off warp by warp, as in wide_body
+    const int pred = g == 0 ? a.ngroups - 1 : g - 1;
+    constexpr int NW = T / 32;
+    static_assert(T % 32 == 0 && NW <= kWarpFlags, "whole warps, one flag each");
+    const int warp = threadIdx.x >> 5;
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0)
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&a.flags[g * kWarpFlags + warp]), "r"(1u) : "memory");
+    if (g != 0) {
+      if ((threadIdx.x & 31) == 0) {
+        uint32_t *f = &a.flags[pred * kWarpFlags + warp];
+        if (!wait_flag(f)) atomicOr(&s_fault, 1u);
+        *f = 0;
+      }
+      __syncwarp();
+    } else {
+      sync();
+      if (threadIdx.x == 0) {
+        for (int w = 0; w < NW; ++w) {
+          uint32_t *f = &a.flags[pred * kWarpFlags + w];
+          if (!wait_flag(f)) s_fault |= 1u;
+          *f = 0;
+        }
+      }
+      sync();
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int m1 = t + r * TR;
+      const double cin = row > 0 ? sm[(row - 1) * RS + m1].y
+                                 : __ldcg(&gcd[(size_t)pred * W + (g == 0 ? (m1 == 0 ? W - 1 : m1 - 1) : m1)]);
+      const int D = a.colD[r];
+      const bool n0 = E0 < D, n1 = E1 < D;
+      const int e0 = E0 - D + (n0 ? n : 0);
+      const bool big0 = e0 < bb;
+      const double P0 = big0 ? p2hi : p2lo, I0 = big0 ? ip2hi : ip2lo;
+      const double pk = ks[r * TR].x;
+      const double d1p = rnd_int(pk * 0x1p-24), l0 = fma(-d1p, 0x1p24, pk);
+      const double tt0 = l0 + cin;
+      const double k0 = rnd_int(tt0 * I0);
+      const double d0 = fma(-k0, P0, tt0);
+      const double d1 = d1p + k0;
+      if (MODE == WIDE_REPORT) {
+        const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
+        a.xint[j0] = (int32_t)d0;
+        a.xint[j0 + 1] = (int32_t)d1;
+      }
+      x[r] = make_double2(d0 * (W0 * (n0 ? a.colS2[r] : a.colS[r])), d1 * (W1 * (n1 ? a.colS2[r] : a.colS[r])));
+    }
+  } else {
+    cp_async_wait_all();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int m1 = t + r * TR;
+      const int D = a.colD[r];
+      const bool n0 = E0 < D, n1 = E1 < D;
+      const uint32_t j0 = 2u * ((uint32_t)m1 * (uint32_t)H + (uint32_t)m2);
+      x[r] = make_double2((double)a.xint[j0] * (W0 * (n0 ? a.colS2[r] : a.colS[r])),
+                          (double)a.xint[j0 + 1] * (W1 * (n1 ? a.colS2[r] : a.colS[r])));
+    }
+  }
+  // forward row transform: the first stage from registers (its barrier
+  // orders the carry reads above before the row is rewritten), the last
+  // straight to global memory
+  double2 *dst = a.A + m2;
+  auto ld_reg = [&](int, int, int r) { return x[r]; };
+  auto st_last = [&](int e, int, int, double2 v) { dst[(size_t)e * H] = v; };
+  fall_stages<P, 0, 1, TR, +1, true, false>(stw, t, sync, ld_reg, st_last, ld, st);
+  if (MODE != WIDE_INIT) {
+    float em = (float)emax;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) em = fmaxf(em, __shfl_xor_sync(0xffffffffu, em, o));
+    if ((threadIdx.x & 31) == 0) s_err[threadIdx.x >> 5] = em;
+    if (out_of_range) atomicOr(&s_fault, 2u);
+    sync();
+    if (threadIdx.x == 0) {
+      float m = 0.f;
+      for (int i = 0; i < (T + 31) / 32; ++i) m = fmaxf(m, s_err[i]);
+      atomicMax(&a.st->err_bits, __float_as_uint(m));
+      if (s_fault) atomicOr(&a.st->fault, s_fault);
+    }
+  }
+}
+
+template <class P, int G>
+__host__ __device__ constexpr int wide_any_threads() { return G * (P::L / P::a[0]); }
+
+template <class P, int G, int MINB, int MODE>
+__global__ void __launch_bounds__(wide_any_threads<P, G>(), MINB) wide_any(WideArgs a) {
+  wide_any_body<P, G, MODE, false>(a, 0);
+}
+
 // ---- batched launches: one launch runs a pass for every member of a length
 // class (members of one FFT length share the kernel); blockIdx.x = member *
 // units + unit.  A member's arguments are copied from the class's device
@@ -922,6 +1125,14 @@ __global__ void __launch_bounds__(wide_threads<P, G>(), min_blocks(wide_threads<
   const int m = blockIdx.x / units;
   const WideArgs &a = member_args(arr, m, &sa);
   wide_body<P, G, WIDE_ITER, true>(a, blockIdx.x - m * units);
+}
+
+template <class P, int G, int MINB>
+__global__ void __launch_bounds__(wide_any_threads<P, G>(), MINB) wide_any_batch(const WideArgs *arr, int units) {
+  __shared__ __align__(16) WideArgs sa;
+  const int m = blockIdx.x / units;
+  const WideArgs &a = member_args(arr, m, &sa);
+  wide_any_body<P, G, WIDE_ITER, true>(a, blockIdx.x - m * units);
 }
 
 // ---- fused iterations for short lengths ---------------------------------

@@ -26,6 +26,7 @@ LL_KERNELS_FUSED = 2
 LL_KERNELS_NO_PREFETCH = 4
 LL_KERNELS_NO_CLUSTER = 8
 LL_KERNELS_CLUSTER8 = 16
+LL_KERNELS_ALT_WIDE = 32
 
 
 class Tuning(ctypes.Structure):

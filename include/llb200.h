@@ -76,6 +76,8 @@ typedef struct {
 #define LL_KERNELS_NO_PREFETCH 4  /* no L2 prefetch of the next wave's data */
 #define LL_KERNELS_NO_CLUSTER 8   /* no cluster-resident iterations */
 #define LL_KERNELS_CLUSTER8 16    /* clusters of at most 8 CTAs */
+#define LL_KERNELS_ALT_WIDE 32    /* the alternative row kernel where a length has one
+                                     (rows in shared memory, 8 elements per thread) */
 
 /* Creates a context for exponent q at FFT length n (FP64 words) on `device`.
  * Replaces alloc_gpu_mem + write_gpu_data (CUDALucas.cu:1096, :1125).

@@ -327,3 +327,28 @@ def test_cluster_variants_agree(tuning):
     assert s1["cluster"] and s0["cluster"]
     assert o1 == o0 and np.array_equal(d1, d0)
     assert cl.digits_res64(d1, q, n, o1) == exact.res64(q, 500)
+
+
+@pytest.mark.parametrize("n", [2097152, 3276800])
+def test_alternative_row_kernel_agrees(n):
+    """The alternative row kernel (rows in shared memory, 8 elements per
+    thread: 1024 = 8x4x4x8, 1280 = 8x4x5x8) gives the digits of the
+    default row kernel and the oracle's residue."""
+    q = _exponent_at(n)
+    off = q // 7
+    d1, o1, e1, s1 = engine_run(q, n, off, 300, kernels=cl.native.LL_KERNELS_ALT_WIDE)
+    d2, o2, e2, s2 = engine_run(q, n, off, 300)
+    assert s1["W"] == s2["W"] and s1["threads_wide"] != s2["threads_wide"], (s1, s2)
+    assert o1 == o2 and np.array_equal(d1, d2)
+    assert e1 < 0.4 and e1 <= 1.5 * e2 + 1e-3 and e2 <= 1.5 * e1 + 1e-3, (e1, e2)
+    from oracle.binding import set_threads
+    set_threads(16)
+    try:
+        o = Oracle(q, n)
+        o.start(off)
+        o.step(8)
+        want = o.res64()
+    finally:
+        set_threads(1)
+    d3, o3, _, _ = engine_run(q, n, off, 8, kernels=cl.native.LL_KERNELS_ALT_WIDE)
+    assert cl.digits_res64(d3, q, n, o3) == want
