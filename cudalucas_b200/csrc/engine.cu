@@ -444,6 +444,7 @@ using C28 = RList<4, 7>;
 using C100 = RList<10, 10>;
 using C112 = RList<16, 7>;
 using C120 = RList<12, 10>;
+using C128 = RList<16, 8>;
 using C140 = RList<14, 10>;
 using C160 = RList<16, 10>;
 using C168 = RList<14, 12>;
@@ -503,7 +504,8 @@ static const StaticTall kTall[] = {
     LLB_TALL(L2048), LLB_TALL(L2304), LLB_TALL(L2560), LLB_TALL(L3072), LLB_TALL(L3584), LLB_TALL(L4096),
     LLB_TALL_ANY(C24, 6, 1),        LLB_TALL_ANY(C28, 7, 1),
     LLB_TALL_ANY(C100, 10, 1),      LLB_TALL_ANY(C112, 8, 1),
-    LLB_TALL_ANY(C120, 12, 1),      LLB_TALL_ANY(C140, 14, 1),
+    LLB_TALL_ANY(C120, 12, 1),      LLB_TALL_ANY(C128, 16, 2),
+    LLB_TALL_ANY(C140, 14, 1),
     LLB_TALL_ANY(C160, 16, 1),      LLB_TALL_ANY(C168, 14, 1),
     LLB_TALL_ANY(C192, 16, 1),      LLB_TALL_ANY(C224, 16, 1),
     LLB_TALL_ANY(C240, 24, 1),      LLB_TALL_ANY(C252, 28, 1),

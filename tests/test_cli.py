@@ -277,8 +277,14 @@ def test_cli_cufftbench_writes_the_gpu_tables_and_they_are_read(cli, tmp_path):
     shapes = (tmp_path / ("%s shapes.txt" % gpu)).read_text().split("\n")
     assert any(l.split()[:1] == ["12"] for l in shapes if l and l[0] != "#")
     kept = [int(k) for k, _, _ in rows]
-    # M216091's default length is 14K; with the table it is the smallest kept length >= its lower bound
-    want = min(k for k in kept if k * 1024 >= cl.fft_bounds(216091)[0])
+    # the table merged as init_ffts merges fft.txt (built-in lengths below the first kept
+    # one and above the last stay), then the length policy's choice for M216091
+    cl.fft_table_merge([k * 1024 for k in kept])
+    try:
+        want = cl.choose_fft_length(216091) // 1024
+    finally:
+        cl.fft_table_merge([])
+    assert want in kept or want < min(kept)
     (tmp_path / "CUDALucas.ini").write_text(INI.replace("ReportIterations=10000", "ReportIterations=100"))
     rc, out, err = run_until([cli, "216091"], tmp_path, "Iteration 200 ")
     assert "Starting M216091 fft length = %dK" % want in out, out[:500]
