@@ -80,8 +80,8 @@ struct TallArgs {
 };
 
 // Ready flags per wide-pass CTA: the specialised kernels hand the carry over
-// warp by warp (at most 16 warps per CTA); the generic ones use the first.
-constexpr int kWarpFlags = 16;
+// warp by warp (at most 32 warps per CTA); the generic ones use the first.
+constexpr int kWarpFlags = 32;
 
 struct WideArgs {
   double2 *A;
@@ -474,6 +474,8 @@ using C2744 = RList<14, 14, 14>;
 // shared memory.  Measured (ms/iter, alternative against default): 2048K
 // 0.0435 / 0.0366, 3200K 0.0679 / 0.0629, 3136K 0.0643 / 0.0650, 1440K
 // 0.0382 / 0.0418.
+// Rows of 2048 (8x4x8x8) and 3072 (8x6x8x8) measured slower too: 12288K
+// 0.2730 / 0.2560, 18432K 0.4102 / 0.3775; they are not compiled.
 using A1280 = RList<8, 4, 5, 8>;  // 160 threads per row, 8 elements each
 using A1024 = RList<8, 4, 4, 8>;
 static const StaticWide kWide[] = {

@@ -332,8 +332,8 @@ def test_cluster_variants_agree(tuning):
 @pytest.mark.parametrize("n", [2097152, 3276800])
 def test_alternative_row_kernel_agrees(n):
     """The alternative row kernel (rows in shared memory, 8 elements per
-    thread: 1024 = 8x4x4x8, 1280 = 8x4x5x8) gives the digits of the
-    default row kernel and the oracle's residue."""
+    thread: 1024 = 8x4x4x8, 1280 = 8x4x5x8) gives the digits of the default
+    row kernel and the oracle's residue."""
     q = _exponent_at(n)
     off = q // 7
     d1, o1, e1, s1 = engine_run(q, n, off, 300, kernels=cl.native.LL_KERNELS_ALT_WIDE)
