@@ -20,16 +20,18 @@
 //     row buffers, unweights, rounds, subtracts 2 and splits the carries
 //     (the wide_static arithmetic); the carries of its last row are stored
 //     into the carry row of the next CTA;
-//   * cluster barrier;
-//   * the first row of each CTA takes those carries (rank 0 the carries of
-//     row H-1, shifted by one element: the 2^q == 1 wrap), the digits are
-//     reweighted and transformed forward, and the last stage stores every
-//     element straight into the column buffer of its column owner;
+//   * the first row of each CTA waits for those carries (rank 0 the carries
+//     of row H-1, shifted by one element: the 2^q == 1 wrap) on an mbarrier
+//     that the previous CTA arrives on once it has stored them (a pairwise
+//     hand-off, not a cluster barrier); the digits are reweighted and
+//     transformed forward, and the last stage stores every element straight
+//     into the column buffer of its column owner;
 //   * cluster barrier.
 //
 // Every transfer between CTAs is a store into the other CTA's shared memory
 // (no remote loads, whose latency would sit on the critical path); the
-// barrier that follows makes it visible.  A row is short and its pass
+// cluster barrier that follows, or for the carries the mbarrier arrive with
+// release semantics, makes it visible.  A row is short and its pass
 // latency bound, so it is spread over TWR threads (a few elements each) and
 // transformed in shared memory with a radix list of small radices (Stockham
 // stages, natural order in and out); the elements a thread rounds and
@@ -91,6 +93,40 @@ __device__ __forceinline__ uint32_t udiv_est(unsigned long long x, uint32_t d, d
   return (uint32_t)e;
 }
 
+// Point-to-point hand-off between two CTAs of the cluster through an
+// mbarrier in the receiver's shared memory: the sender's stores into the
+// receiver, a CTA barrier, then one release arrive on the receiver's
+// barrier; the receiver waits with acquire at cluster scope.  The wait is
+// bounded: on expiry it returns false (the caller sets the timeout fault bit
+// and goes on, so every later barrier is still taken).
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ uint32_t mbar_remote(uint64_t *bar, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_addr(bar)), "r"(rank));
+  return a;
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t remote) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote) : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_addr(bar);
+  for (int k = 0; k < (1 << 22); ++k) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // Column k1 held in local column slot lc of CTA `rank`.
 template <class CF>
 __device__ __forceinline__ int cluster_col_k1(int rank, int lc) {
@@ -119,6 +155,7 @@ __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
   extern __shared__ double2 sm[];
   __shared__ float s_err[32];
   __shared__ uint32_t s_fault;
+  __shared__ __align__(8) uint64_t s_cbar;  // the previous CTA's carries have arrived
   const int rank = (int)cl.block_rank();
   const int tid = threadIdx.x;
   double2 *rows = sm;
@@ -129,7 +166,10 @@ __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
   double *cin = reinterpret_cast<double *>(sm + CF::o_cin);
 
   // ---- set-up: tables, twiddles of the owned columns, the owned state
-  if (tid == 0) s_fault = 0;
+  if (tid == 0) {
+    s_fault = 0;
+    mbar_init(&s_cbar, 1);  // one arrive per iteration: the previous CTA's
+  }
   for (int i = tid; i < tw_size<PR>(); i += T) stw[i] = stwr[i];
   for (int i = tid; i < tw_size<PT>(); i += T) stt[i] = stwr[tw_size<PR>() + i];
   for (int i = tid; i < W; i += T) {
@@ -174,6 +214,7 @@ __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
   // shifted by one element)
   const bool wrap = rank == CF::ROWCTAS - 1;
   double *next_cin = cl.map_shared_rank(cin, (unsigned)(wrap ? 0 : rank + 1));
+  const uint32_t next_cbar = mbar_remote(&s_cbar, (unsigned)(wrap ? 0 : rank + 1));
   uint32_t off = ta.st->offset;
   double emax = 0.0;
   bool out_of_range = false;
@@ -290,9 +331,15 @@ __global__ void __launch_bounds__(ClusterCfg<PR, TWR, PT, TC, C, RPC>::T, 1)
         rw[m1] = make_double2(fma(d1p, 0x1p24, l0), co);
         if (row == RPC - 1) next_cin[wrap ? (m1 + 1 == W ? 0 : m1 + 1) : m1] = co;
       }
+      // the carries of this CTA's rows are in place (the next row reads them
+      // below); those of the last row go to the next CTA with one release
+      syncW();
+      if (tid == 0) mbar_arrive_remote(next_cbar);
     }
-    cl.sync();  // carries of every CTA's last row delivered
     if (wide) {
+      // the first row waits for the previous CTA's carries (the only
+      // dependence between CTAs inside the wide pass)
+      if (row == 0 && !mbar_wait(&s_cbar, it & 1u)) atomicOr(&s_fault, 1u);
       const bool last_it = report && it + 1 == iters;
       double2 x[EPR];
 #pragma unroll
