@@ -447,7 +447,8 @@ def run_batch(args, world, rank, local):
     qs, ns = zip(*members)
     offs = [(q * 7) // 11 for q in qs]
     S, K, W = args.iters_per_step, args.steps, args.warmup
-    b = cl.LLBatch(qs, ns, device=local, graph_iters=args.batch_graph_iters, by_length=args.batch_by_length)
+    by_length = not args.batch_per_member
+    b = cl.LLBatch(qs, ns, device=local, graph_iters=args.batch_graph_iters, by_length=by_length)
     classes = b.classes
     b.start(offs)
     b.step(S, report=True)           # the first warm-up step, checked against solo runs below
@@ -471,7 +472,7 @@ def run_batch(args, world, rank, local):
     other = None
     if args.batch_compare:
         # the other launch mode over the same members and steps
-        b2 = cl.LLBatch(qs, ns, device=local, graph_iters=args.batch_graph_iters, by_length=not args.batch_by_length)
+        b2 = cl.LLBatch(qs, ns, device=local, graph_iters=args.batch_graph_iters, by_length=not by_length)
         b2.start(offs)
         for _ in range(W):
             b2.step(S)
@@ -516,7 +517,7 @@ def run_batch(args, world, rank, local):
         "config": {"workload": "batch: %d primes log-uniform in [1e6, 2e7] (seed 7), lengths %dK..%dK"
                                % (len(members), min(ns) // 1024, max(ns) // 1024),
                    "iters_per_step": S, "graph_iters": args.batch_graph_iters,
-                   "launches": "one per pass per length class (%d classes)" % classes if args.batch_by_length
+                   "launches": "one per pass per length class (%d classes)" % classes if by_length
                                else "one per pass per member",
                    "serial_iter_s": round(serial_ips, 1), "speedup_vs_serial": round(batch_ips / serial_ips, 3),
                    "serial_sample": "%d iterations of each exponent alone, from the batch's offsets" % Ss,
@@ -526,7 +527,7 @@ def run_batch(args, world, rank, local):
         "res64_checked": {"against": "each member run alone for the same %d iterations" % S,
                           "members": len(members) if Ss == S else 0, "mismatched": mismatched},
         "clocks": clk.summary(),
-        "gpu_launches": 2 * len(members) * K * S,
+        "gpu_launches": 2 * (classes if by_length else len(members)) * K * S,
     }
 
 
@@ -590,8 +591,8 @@ def main():
     ap.add_argument("--serve-hbm-gb", type=float, default=150.0)
     ap.add_argument("--batch-compare", action="store_true",
                     help="also time the other launch mode (per member / per length class)")
-    ap.add_argument("--batch-by-length", action="store_true",
-                    help="launch each pass once per length class instead of once per member")
+    ap.add_argument("--batch-per-member", action="store_true",
+                    help="launch each member's passes on their own instead of once per length class")
     ap.add_argument("--iters-per-step", type=int, default=10000)
     ap.add_argument("--cpu-iters", type=int, default=20,
                     help="oracle iterations on one host thread for cpu_baseline (0: skip)")

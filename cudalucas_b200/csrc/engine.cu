@@ -570,6 +570,12 @@ struct ClusterKernel {
 // stage) or 32 threads per row
 using R256A = RList<4, 4, 4, 4>;
 using R256B = RList<8, 4, 8>;
+// rows of 768 and 1024: 192 and 256 threads per row (both directions run the
+// list in the same order, so it need not be palindromic)
+using R768 = RList<4, 6, 8, 4>;
+using R1024 = RList<4, 8, 8, 4>;
+using R768B = RList<8, 12, 8>;    // 96 threads per row
+using R1024B = RList<8, 16, 8>;   // 128 threads per row
 // column lists of small radices: many threads per column, short chains
 using K16 = RList<4, 4>;
 using K20 = RList<4, 5>;
@@ -583,9 +589,10 @@ using K112 = RList<4, 4, 7>;
 // Only lengths where one cluster (16 SMs) beats two launches over the whole
 // GPU (us per iteration, cluster against two launches): 8K 3.6 / 13.4, 10K
 // 5.1 / 15.6, 12K 4.8 / 9.9, 14K 5.7 / 10.0, 16K 4.8 / 17.2, 18K 6.1 / 17.7,
-// 20K 6.5 / 16.3, 32K 7.8 / 16.5, 56K 13.1 / 14.8.  At 50K (15.7 / 11.7) and
-// 96K (21.7 / 12.1) the arithmetic of 16 SMs is the bound and the two-launch
-// path stays.  The entries cover shapes with rows of 256 only.
+// 20K 6.5 / 16.3, 32K 7.8 / 16.5, 56K 13.1 / 14.8, and with rows of 768 and
+// 1024: 36K 11.6 / 16.1, 42K 12.9 / 16.3, 48K 14.5 / 21.7.  At 50K (15.7 /
+// 11.7) and 96K (21.7 / 12.1) the arithmetic of 16 SMs is the bound and the
+// two-launch path stays.
 static const ClusterKernel kCluster[] = {
     LLB_CLUSTER(R256A, 64, K16, 4, 16, 1),    LLB_CLUSTER(R256B, 32, K20, 5, 16, 2),
     LLB_CLUSTER(R256A, 64, K24, 6, 16, 2),    LLB_CLUSTER(R256B, 32, K24, 6, 16, 2),
@@ -593,6 +600,9 @@ static const ClusterKernel kCluster[] = {
     LLB_CLUSTER(R256A, 64, K28, 7, 8, 4),     LLB_CLUSTER(R256A, 64, K32, 8, 16, 2),
     LLB_CLUSTER(R256B, 32, K36, 6, 16, 3),    LLB_CLUSTER(R256A, 64, K40, 8, 16, 4),
     LLB_CLUSTER(R256A, 64, K64, 16, 16, 4),   LLB_CLUSTER(R256B, 32, K112, 28, 16, 8),
+    LLB_CLUSTER(R768, 192, K24, 6, 16, 2),    LLB_CLUSTER(R768B, 96, K24, 6, 16, 2),
+    LLB_CLUSTER(R768B, 96, K28, 8, 16, 2),    LLB_CLUSTER(R768, 192, K28, 8, 16, 2),
+    LLB_CLUSTER(R1024B, 128, K24, 6, 16, 2),  LLB_CLUSTER(R1024, 256, K24, 6, 16, 2),
 };
 
 static const StaticTall *find_tall(int L) {
@@ -1807,7 +1817,7 @@ struct ll_batch {
   cudaStream_t stream = nullptr;
   std::vector<cudaEvent_t> events;  // [0] fork, [1..] joins
   int graph_iters = 0;
-  bool by_class = false;                // one launch per pass per length class (else per member)
+  bool by_class = true;                 // one launch per pass per length class (else per member)
   std::vector<BatchClass> classes;
   std::vector<int> singles;             // members launched on their own
   cudaGraph_t graph = nullptr;

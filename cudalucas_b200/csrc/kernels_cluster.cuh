@@ -77,7 +77,6 @@ struct ClusterCfg {
   static_assert(W % TWR == 0 && TWR % 32 == 0, "whole warps per row");
   static_assert(H % RPC == 0 && ROWCTAS <= C, "whole row groups, at most one per CTA");
   static_assert(TT == T || TT % 32 == 0, "a tall pass on part of the CTA needs whole warps");
-  static_assert(palindromic<PR>(), "inverse stages reuse the forward twiddle table");
   static_assert(PR::N <= 4, "the host keeps four radices of the row list");
   static_assert(W / PR::a[0] == TWR && W / PR::a[PR::N - 1] == TWR,
                 "first and last row stages: one butterfly per thread, elements t + j*TWR");

@@ -137,7 +137,7 @@ class LLContext:
 class LLBatch:
     """Many exponents advancing together (ll_batch_* in include/llb200.h)."""
 
-    def __init__(self, qs, ns, device=0, graph_iters=10, by_length=False):
+    def __init__(self, qs, ns, device=0, graph_iters=10, by_length=True):
         L = native.lib()
         self.qs = [int(x) for x in qs]
         self.ns = [int(x) for x in ns]
@@ -149,8 +149,7 @@ class LLBatch:
         if rc:
             raise LLError(rc, "ll_batch_create")
         self._keep = (q, n)
-        if by_length:
-            L.ll_batch_group_by_length(self._h, 1)
+        L.ll_batch_group_by_length(self._h, 1 if by_length else 0)
 
     @property
     def classes(self):

@@ -67,7 +67,7 @@ typedef struct {
  * (measured slower at 12K and 14K, equal at 56K, so not the default);
  * LL_KERNELS_NO_PREFETCH turns off the L2 prefetch that lengths larger than
  * L2 use.  Short lengths with a cluster-resident kernel (8K, 10K, 12K, 14K,
- * 16K, 18K, 20K, 32K, 56K) run each ll_step as one launch of one thread-block cluster whose
+ * 16K, 18K, 20K, 32K, 36K, 42K, 48K, 56K) run each ll_step as one launch of one thread-block cluster whose
  * shared memory holds the whole state; LL_KERNELS_NO_CLUSTER turns that off
  * (two launches per iteration), LL_KERNELS_CLUSTER8 keeps to the portable
  * cluster size of 8 CTAs. */
@@ -185,12 +185,13 @@ ll_status ll_batch_step(ll_batch *b, uint32_t iters, uint32_t flags, float *max_
 ll_status ll_batch_sync(ll_batch *b);
 void *ll_batch_stream(const ll_batch *b);  /* stream the step graphs run on */
 /* Members of one FFT length whose passes have specialised kernels form a
- * length class.  on = 1 makes one launch per pass run the pass for every
- * member of the class (the step graph then has one branch per class, 2
- * kernel nodes per iteration); the default, on = 0, launches every member's
- * passes separately (one branch per member), which measured about 5 %
- * faster on the 256-exponent benchmark set.  Call before the first
- * ll_batch_step.  ll_batch_classes gives the number of length classes. */
+ * length class.  on = 1 (the default) makes one launch per pass run the pass
+ * for every member of the class (the step graph then has one branch per
+ * class, 2 kernel nodes per iteration); on = 0 launches every member's
+ * passes separately (one branch per member).  On the 256-exponent
+ * benchmark set the two measured 143.6 K and 141.2 K iterations/s.  Call
+ * before the first ll_batch_step.  ll_batch_classes gives the number of
+ * length classes. */
 ll_status ll_batch_group_by_length(ll_batch *b, int32_t on);
 int32_t ll_batch_classes(const ll_batch *b);
 ll_status ll_batch_res64(ll_batch *b, uint64_t *res64);

@@ -292,7 +292,7 @@ def test_fused_iterations_equal_two_launch_iterations(n):
     assert cl.digits_res64(d1, q, n, o1) == o.res64()
 
 
-@pytest.mark.parametrize("n", [8192, 10240, 12288, 14336, 16384, 18432, 20480, 32768, 57344])
+@pytest.mark.parametrize("n", [8192, 10240, 12288, 14336, 16384, 18432, 20480, 32768, 36864, 43008, 49152, 57344])
 def test_cluster_iterations_equal_two_launch_iterations(n):
     """Short lengths run every step as one launch of one thread-block
     cluster whose shared memory holds the state (cluster_iters).  After many
