@@ -1435,6 +1435,12 @@ uint64_t ll_context_bytes(uint32_t q, uint32_t n, const ll_tuning *tuning) {
   b += 20 * 2 * H + 20 * W;                                                           // weights
   if (s.sw) b += 16 * (uint64_t)s.sw->extra;
   if (s.st) b += 16 * (uint64_t)s.st->tw;
+  // the cluster kernel's stage twiddles, when the length has one (the
+  // largest table among its variants)
+  uint64_t tw_cluster = 0;
+  for (const auto &k : kCluster)
+    if (k.W == s.W && k.H == s.H) tw_cluster = std::max<uint64_t>(tw_cluster, 16 * (uint64_t)k.tw);
+  b += tw_cluster;
   return b;
 }
 
