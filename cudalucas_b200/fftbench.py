@@ -1,9 +1,10 @@
 """Times the engine per FFT length and launch shape: the engine's counterpart
 of CUDALucas's -cufftbench / -threadbench modes (CUDALucas.cu:2413, :2144),
 which time cuFFT and the reference kernels and write `<gpu> fft.txt` /
-`<gpu> threads.txt`.  Here every candidate shape (row width W, rows per CTA
-G) of each length is timed with CUDA events on the context's stream, and the
-fastest is printed (and optionally written as a tuning table).
+`<gpu> threads.txt`.  Here every launch choice of each length (row width W,
+kernel variants; see candidate_shapes) is timed with CUDA events on the
+context's stream, and the fastest is printed (and optionally written as a
+tuning table).
 
   python -m cudalucas_b200.fftbench 3200K [18432K ...] [--iters 200]
          [--width W] [--rows G] [--kernels FLAGS] [--all-shapes] [--table FILE]
@@ -92,19 +93,34 @@ def time_shape(q, n, iters, tuning=None, device=0):
 
 
 def candidate_shapes(n):
+    """The launch choices the engine offers for length n: every row width W
+    with the engine's own kernels for it (specialised where they exist, rows
+    per CTA chosen by the engine), and for the default width the kernel
+    variants (two launches instead of the cluster-resident step, the
+    alternative row kernel).  Setting rows per CTA would force the generic
+    kernels, so it is not a candidate."""
     N = n // 2
-    out = []
+    out, seen = [], set()
+    q = exponent_for(n)
+
+    def add(t):
+        try:
+            c = engine.LLContext(q, n, tuning=t)
+        except engine.LLError:
+            return
+        sh = c.shape
+        c.close()
+        key = (sh["W"], sh["G"], sh["threads_wide"], sh["threads_tall"], sh.get("cluster"))
+        if key not in seen:
+            seen.add(key)
+            out.append((t, sh))
+
+    add(None)
+    add({"kernels": native.LL_KERNELS_NO_CLUSTER})
+    add({"kernels": native.LL_KERNELS_ALT_WIDE})
     for w in range(16, 8193, 2):
-        if N % w:
-            continue
-        for g in (1, 2, 4, 8):
-            t = {"width": w, "rows_per_cta": g}
-            try:
-                c = engine.LLContext(exponent_for(n), n, tuning=t)
-            except engine.LLError:
-                continue
-            out.append((t, c.shape))
-            c.close()
+        if N % w == 0:
+            add({"width": w})
     return out
 
 
