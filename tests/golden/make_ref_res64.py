@@ -13,8 +13,8 @@ no fft.txt/threads.txt of an earlier run can change the FFT length:
 It also records the reference's kernel-only timing, `-cufftbench L L 20`
 (CUDALucas.cu:2440-2500), for the three lengths.
 
-Needs a GPU; writes to --out (default: this folder).  Example, on a GPU box:
-  python tests/golden/make_ref_res64.py --out gpurun_out/golden
+Needs a GPU; writes to --out (default: this folder).  Example:
+  python tests/golden/make_ref_res64.py --out /tmp/golden
 """
 import argparse
 import json
