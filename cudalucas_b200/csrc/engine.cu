@@ -454,6 +454,7 @@ using C240 = RList<12, 10, 2>;
 using C252 = RList<14, 9, 2>;
 using C288 = RList<16, 9, 2>;
 using C320 = RList<16, 10, 2>;
+using C324 = RList<4, 9, 9>;
 using C336 = RList<14, 12, 2>;
 using C360 = RList<10, 9, 4>;
 using C392 = RList<14, 14, 2>;
@@ -511,7 +512,7 @@ static const StaticTall kTall[] = {
     LLB_TALL_ANY(C160, 16, 1),      LLB_TALL_ANY(C168, 14, 1),
     LLB_TALL_ANY(C192, 16, 1),      LLB_TALL_ANY(C224, 16, 1),
     LLB_TALL_ANY(C240, 24, 1),      LLB_TALL_ANY(C252, 28, 1),
-    LLB_TALL_ANY(C288, 32, 2),      LLB_TALL_ANY(C320, 32, 2),
+    LLB_TALL_ANY(C288, 32, 2),      LLB_TALL_ANY(C320, 32, 2),      LLB_TALL_ANY(C324, 81, 1),
     LLB_TALL_ANY(C336, 28, 2),      LLB_TALL_ANY(C360, 40, 2),
     LLB_TALL_ANY(C392, 28, 2),      LLB_TALL_ANY(C400, 40, 2),
     LLB_TALL_ANY(C448, 32, 2),      LLB_TALL_ANY(C576, 48, 2),

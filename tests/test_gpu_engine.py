@@ -248,7 +248,7 @@ def _exponent_at(n, bits=17.6):
     return q
 
 
-@pytest.mark.parametrize("nk", [12, 14, 50, 56, 60, 64, 70, 80, 96, 112, 120, 126, 144, 160, 180, 224, 288, 320, 336,
+@pytest.mark.parametrize("nk", [12, 14, 50, 56, 60, 64, 70, 80, 96, 112, 120, 126, 144, 160, 162, 180, 224, 288, 320, 336,
                                 360, 392, 400, 448, 576, 864, 900, 3136])
 def test_specialised_columns_of_any_radix_list(nk):
     """Lengths whose columns are not 16 x M x 16 (C1's 12K, the batch set's
