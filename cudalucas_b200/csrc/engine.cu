@@ -420,6 +420,11 @@ struct StaticTall {
 #define LLB_TALL(LIST) \
   {LIST::L, tall_static<LIST>, tall_static_batch<LIST>, LLB_RAD(LIST), tw_size<LIST>(),                      \
    padded(2 * LIST::L) + tall_extra<LIST>(), 2 * (LIST::L / 16), 1}
+// the same without the batched variant (lengths that batches leave to
+// solo launches: members without one run on their own branch)
+#define LLB_TALL_ANY_SOLO(LIST, TC, PP)                                                                  \
+  {LIST::L, tall_any<LIST, TC, PP>, nullptr, LLB_RAD(LIST), tw_size<LIST>(),                               \
+   tall_any_smem<LIST, PP>(), 2 * PP * TC, PP}
 // any radix list: TC threads per column, PP column pairs per CTA
 #define LLB_TALL_ANY(LIST, TC, PP)                                                                       \
   {LIST::L, tall_any<LIST, TC, PP>, tall_any_batch<LIST, TC, PP>, LLB_RAD(LIST), tw_size<LIST>(),          \
@@ -469,6 +474,29 @@ using C784 = RList<16, 7, 7>;
 using C800 = RList<16, 10, 5>;
 using C1568 = RList<16, 14, 7>;
 using C2744 = RList<14, 14, 14>;
+// columns of the long lengths (6048K and up): four stages at most, up to 486
+// threads per column
+using C1620 = RList<3, 9, 10, 6>;
+using C1728 = RList<12, 12, 12>;
+using C1800 = RList<5, 5, 12, 6>;
+using C1944 = RList<3, 9, 12, 6>;
+using C2160 = RList<5, 12, 6, 6>;
+using C2240 = RList<14, 16, 10>;
+using C2352 = RList<14, 14, 12>;
+using C2400 = RList<5, 5, 16, 6>;
+using C2592 = RList<3, 12, 12, 6>;
+using C2688 = RList<14, 16, 12>;
+using C2800 = RList<5, 5, 14, 8>;
+using C2880 = RList<5, 12, 12, 4>;
+using C2916 = RList<9, 9, 6, 6>;
+using C3024 = RList<3, 14, 12, 6>;
+using C3200 = RList<5, 5, 16, 8>;
+using C3402 = RList<3, 9, 9, 14>;
+using C3500 = RList<5, 7, 10, 10>;
+using C3888 = RList<9, 12, 6, 6>;
+using C4000 = RList<10, 10, 10, 4>;
+using C4050 = RList<5, 9, 9, 10>;
+using C4374 = RList<9, 9, 9, 6>;
 
 // Alternative row kernels (opt-in, LL_KERNELS_ALT_WIDE): twice the warps per
 // SM (64-80 registers, 3 CTAs of 8 or 10 warps) but every stage through
@@ -520,6 +548,27 @@ static const StaticTall kTall[] = {
     LLB_TALL_ANY(C672, 56, 2),      LLB_TALL_ANY(C720, 72, 2),
     LLB_TALL_ANY(C784, 56, 2),      LLB_TALL_ANY(C800, 80, 2),
     LLB_TALL_ANY(C1568, 112, 1),    LLB_TALL_ANY(C2744, 196, 1),
+    LLB_TALL_ANY_SOLO(C1620, 180, 1),
+    LLB_TALL_ANY_SOLO(C1728, 144, 1),
+    LLB_TALL_ANY_SOLO(C1800, 150, 1),
+    LLB_TALL_ANY_SOLO(C1944, 216, 1),
+    LLB_TALL_ANY_SOLO(C2160, 180, 1),
+    LLB_TALL_ANY_SOLO(C2240, 224, 1),
+    LLB_TALL_ANY_SOLO(C2352, 196, 1),
+    LLB_TALL_ANY_SOLO(C2400, 200, 1),
+    LLB_TALL_ANY_SOLO(C2592, 216, 1),
+    LLB_TALL_ANY_SOLO(C2688, 224, 1),
+    LLB_TALL_ANY_SOLO(C2800, 200, 1),
+    LLB_TALL_ANY_SOLO(C2880, 240, 1),
+    LLB_TALL_ANY_SOLO(C2916, 324, 1),
+    LLB_TALL_ANY_SOLO(C3024, 252, 1),
+    LLB_TALL_ANY_SOLO(C3200, 214, 1),
+    LLB_TALL_ANY_SOLO(C3402, 378, 1),
+    LLB_TALL_ANY_SOLO(C3500, 350, 1),
+    LLB_TALL_ANY_SOLO(C3888, 432, 1),
+    LLB_TALL_ANY_SOLO(C4000, 400, 1),
+    LLB_TALL_ANY_SOLO(C4050, 450, 1),
+    LLB_TALL_ANY_SOLO(C4374, 486, 1),
 };
 
 // Fused cooperative kernels (fused_iters) for short lengths: the shape
@@ -1038,7 +1087,8 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
       for (const auto &k : kTall)
         if (e == cudaSuccess &&
             ((e = cudaFuncSetAttribute(k.run, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess ||
-             (e = cudaFuncSetAttribute(k.batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess))
+             (k.batch &&
+              (e = cudaFuncSetAttribute(k.batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)st)) != cudaSuccess)))
           break;
       if (e != cudaSuccess) {
         rc = cuda_fail(ctx, e, "cudaFuncSetAttribute (static)");
@@ -1854,7 +1904,7 @@ static ll_status build_classes(ll_batch *b) {
   std::vector<int> order;
   for (size_t i = 0; i < b->members.size(); ++i) {
     const ll_ctx *c = b->members[i];
-    if (!(c->shape.sw && c->shape.st)) {
+    if (!(c->shape.sw && c->shape.st && c->shape.st->batch)) {
       b->singles.push_back((int)i);
       continue;
     }

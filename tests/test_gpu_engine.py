@@ -352,3 +352,22 @@ def test_alternative_row_kernel_agrees(n):
         set_threads(1)
     d3, o3, _, _ = engine_run(q, n, off, 8, kernels=cl.native.LL_KERNELS_ALT_WIDE)
     assert cl.digits_res64(d3, q, n, o3) == want
+
+
+@pytest.mark.parametrize("nk", [6048, 6480, 7200, 7776, 8640, 10584, 10800, 11200, 12096, 12960, 14400, 17496,
+                                18144, 19600, 20000, 23328, 23814, 24300, 24500, 25600, 26244])
+def test_long_lengths_columns_agree_with_generic_kernels(nk):
+    """The column lengths of the long table lengths (1620-4374, up to four
+    stages of radices <= 16) run tall_any; after a few iterations the digits
+    equal (modulo 2^q-1) those of the generic kernels, and so does Res64."""
+    n = nk * 1024
+    q = _exponent_at(n, 17.3)
+    off = q // 9
+    d1, o1, e1, s1 = engine_run(q, n, off, 6)
+    assert s1["tall_specialised"], s1
+    d2, o2, e2, s2 = engine_run(q, n, off, 6, kernels=cl.native.LL_KERNELS_GENERIC)
+    assert not s2["tall_specialised"]
+    assert o1 == o2
+    assert np.array_equal(cl.standardize(d1, q, n)[0], cl.standardize(d2, q, n)[0])
+    assert cl.digits_res64(d1, q, n, o1) == cl.digits_res64(d2, q, n, o2)
+    assert e1 < 0.4 and e2 < 0.4
