@@ -747,34 +747,47 @@ static std::vector<uint32_t> read_fft_file(const std::string &name) {
 // length from s K to e K (passes x 50 iterations after a warm-up of 50),
 // keeps the lengths faster than every longer one (and the powers of two),
 // writes them to `<gpu> fft.txt`, moving an older file aside as the
-// reference does.  For each length the fastest launch shape among the
-// engine's candidates (row width W) goes to `<gpu> shapes.txt`.
+// reference does.  For each length the fastest launch choice among the
+// engine's candidates (row width W; for the engine's own width also the
+// kernel variants: two launches instead of the cluster-resident step, the
+// alternative row kernel) goes to `<gpu> shapes.txt` as width and
+// ll_tuning.kernels.
 static int cufftbench(const Config &cfg, const char *gpu, int s, int e, int passes) {
   if (!gpu[0]) { fprintf(stderr, "no CUDA device %d\n", cfg.device); return 2; }
   std::vector<uint32_t> lens;
   std::vector<float> times;
-  std::vector<int32_t> widths;
+  std::vector<int32_t> widths, kernels;
   for (int k = s; k <= e; ++k) {
     const uint32_t n = (uint32_t)k * 1024u;
     if (!ll_length_supported(n)) continue;
     uint32_t q = (uint32_t)(n * 17.6) | 1;
     while (!is_prime(q)) q += 2;
     float best = 0.f;
-    int32_t best_w = 0;
-    // candidate row widths: the engine's own choice first, then the
-    // divisors of N = n/2 near its square root
-    std::vector<int32_t> cand = {0};
+    int32_t best_w = 0, best_k = 0;
+    // candidates: the engine's own choice, its kernel variants, then the
+    // divisors of N = n/2 near its square root as row widths
+    std::vector<std::pair<int32_t, int32_t>> cand = {{0, 0}, {0, LL_KERNELS_NO_CLUSTER}, {0, LL_KERNELS_ALT_WIDE}};
     const uint32_t N = n / 2;
     for (uint32_t w = 64; w <= 8192 && w <= N; w += 2)
-      if (N % w == 0 && (double)w * w >= N / 16.0 && (double)w * w <= 16.0 * N) cand.push_back((int32_t)w);
-    for (int32_t w : cand) {
+      if (N % w == 0 && (double)w * w >= N / 16.0 && (double)w * w <= 16.0 * N) cand.push_back({(int32_t)w, 0});
+    int32_t def_w = 0, def_tw = 0, def_kinds = -1;
+    for (const auto &wk : cand) {
+      const int32_t w = wk.first;
       ll_tuning tu{};
       tu.width = w;
+      tu.kernels = wk.second;
       ll_ctx *c = nullptr;
-      if (ll_create(cfg.device, q, n, w ? &tu : nullptr, &c) != LL_OK) continue;
-      int32_t W = 0;
-      ll_shape(c, &W, nullptr, nullptr, nullptr, nullptr);
+      if (ll_create(cfg.device, q, n, (w || wk.second) ? &tu : nullptr, &c) != LL_OK) continue;
+      int32_t W = 0, TW = 0;
+      ll_shape(c, &W, nullptr, nullptr, &TW, nullptr);
+      const int32_t kinds = ll_kernel_kinds(c);
       if (w && w != W) { ll_destroy(c); continue; }
+      if (!w && !wk.second) { def_w = W; def_tw = TW; def_kinds = kinds; }
+      // a variant that changes nothing, or the engine's width again, is not timed twice
+      if ((!w && wk.second && W == def_w && TW == def_tw && kinds == def_kinds) || (w && w == def_w)) {
+        ll_destroy(c);
+        continue;
+      }
       float err = 0.f;
       ll_start(c, 0);
       ll_step(c, 50, LL_ERRCHK, &err);
@@ -783,14 +796,15 @@ static int cufftbench(const Config &cfg, const char *gpu, int s, int e, int pass
       const float ms = (float)((now_s() - t0) * 1000.0 / (50.0 * passes));
       ll_destroy(c);
       if (st != LL_OK) continue;
-      if (best == 0.f || ms < best) { best = ms; best_w = W; }
+      if (best == 0.f || ms < best) { best = ms; best_w = W; best_k = wk.second; }
     }
     if (best == 0.f) continue;
-    printf("fft size = %uK, ave time = %6.4f msec, width %d\n", n / 1024, best, best_w);
+    printf("fft size = %uK, ave time = %6.4f msec, width %d, kernels %d\n", n / 1024, best, best_w, best_k);
     fflush(stdout);
     lens.push_back(n);
     times.push_back(best);
     widths.push_back(best_w);
+    kernels.push_back(best_k);
   }
   std::vector<int32_t> keep(lens.size(), 0);
   ll_fft_prune(lens.data(), times.data(), (int32_t)lens.size(), keep.data());
@@ -805,9 +819,9 @@ static int cufftbench(const Config &cfg, const char *gpu, int s, int e, int pass
   FILE *g = fopen((std::string(gpu) + " shapes.txt").c_str(), "w");
   if (!f) { fprintf(stderr, "Cannot open %s.\n", name.c_str()); return 2; }
   fprintf(f, "Device              %s\n\n  fft    max exp  ms/iter\n", gpu);
-  if (g) fprintf(g, "# fft(K) width ms/iter\n");
+  if (g) fprintf(g, "# fft(K) width ms/iter kernels\n");
   for (size_t i = 0; i < lens.size(); ++i) {
-    if (g) fprintf(g, "%5u %6d %8.4f\n", lens[i] / 1024, widths[i], times[i]);
+    if (g) fprintf(g, "%5u %6d %8.4f %d\n", lens[i] / 1024, widths[i], times[i], kernels[i]);
     if (keep[i]) fprintf(f, "%5u %10u %8.4f\n", lens[i] / 1024, ll_fft_max_exponent(lens[i]), times[i]);
   }
   fclose(f);
@@ -826,10 +840,12 @@ static bool shape_for(const Config &cfg, uint32_t n, ll_tuning &tu) {
   bool found = false;
   while (fgets(buf, sizeof buf, f)) {
     unsigned k = 0;
-    int w = 0;
-    if (buf[0] != '#' && sscanf(buf, "%u %d", &k, &w) == 2 && k * 1024u == n && w > 0) {
+    int w = 0, kern = 0;
+    float ms = 0.f;
+    if (buf[0] != '#' && sscanf(buf, "%u %d %f %d", &k, &w, &ms, &kern) >= 2 && k * 1024u == n && w > 0) {
       tu = ll_tuning{};
       tu.width = w;
+      tu.kernels = kern & (LL_KERNELS_NO_CLUSTER | LL_KERNELS_ALT_WIDE);  // the variants the table may choose
       found = true;
     }
   }

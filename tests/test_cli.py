@@ -275,7 +275,11 @@ def test_cli_cufftbench_writes_the_gpu_tables_and_they_are_read(cli, tmp_path):
     assert rows and all(12 <= int(k) <= 20 for k, _, _ in rows)
     assert ["16" == k for k, _, _ in rows].count(True) == 1      # a power of two is always kept
     shapes = (tmp_path / ("%s shapes.txt" % gpu)).read_text().split("\n")
-    assert any(l.split()[:1] == ["12"] for l in shapes if l and l[0] != "#")
+    rows_s = [l.split() for l in shapes if l and l[0] != "#"]
+    assert any(r[:1] == ["12"] for r in rows_s)
+    # fft(K) width ms/iter kernels: the kernel variant is one the table may choose
+    assert all(len(r) == 4 and int(r[3]) in (0, cl.native.LL_KERNELS_NO_CLUSTER, cl.native.LL_KERNELS_ALT_WIDE)
+               for r in rows_s)
     kept = [int(k) for k, _, _ in rows]
     # the table merged as init_ffts merges fft.txt (built-in lengths below the first kept
     # one and above the last stay), then the length policy's choice for M216091
