@@ -157,9 +157,9 @@ def main(argv=None):
         best = None
         for t in shapes:
             ms, tall, wide, err, shape = time_shape(q, n, args.iters, t, args.device)
-            print("%8dK q=%d W=%d H=%d G=%d%s  %.4f ms/iter  tall %.1f us  wide %.1f us  err %.5f"
+            print("%8dK q=%d W=%d H=%d G=%d%s  %.4f ms/iter  tall %.1f us  wide %.1f us  err %.5f  tuning %s"
                   % (n // 1024, q, shape["W"], shape["H"], shape["G"], " cluster" if shape.get("cluster") else "",
-                     ms, tall, wide, err), flush=True)
+                     ms, tall, wide, err, json.dumps(t or {}, separators=(",", ":"))), flush=True)
             if best is None or ms < best[0]:
                 best = (ms, shape)
         table[n] = {"ms_per_iter": best[0], **best[1]}
