@@ -874,6 +874,78 @@ std::vector<double2> stage_twiddles(const int *rad, int nrad) {
 
 }  // namespace
 
+// Launch preferences measured on the B200 for lengths of the reference's
+// table where the engine's default shape (row width nearest sqrt(N)) is not
+// the fastest: the row width and ll_tuning.kernels to use when the caller
+// gives no tuning.  A `<gpu> shapes.txt` from llucas -cufftbench, or any
+// explicit tuning, takes precedence.
+struct PreferredShape {
+  uint32_t n;       // FFT length in words
+  int32_t width;    // row width W
+  int32_t kernels;  // LL_KERNELS_* flags
+};
+// (fftbench --all-shapes over the table lengths, 200 iterations timed with
+// CUDA events; kept where the preference is at least 8 % faster)
+static const PreferredShape kPreferred[] = {
+    {288u * 1024, 256, 0},  // 288K: 0.0159 against 0.0220 ms/iter (W = 512)
+    {324u * 1024, 256, 0},  // 324K: 0.0176 against 0.0227 ms/iter (W = 512)
+    {336u * 1024, 768, 0},  // 336K: 0.0175 against 0.0243 ms/iter (W = 512)
+    {360u * 1024, 768, 0},  // 360K: 0.0181 against 0.0254 ms/iter (W = 512)
+    {392u * 1024, 256, 0},  // 392K: 0.0183 against 0.0255 ms/iter (W = 512)
+    {400u * 1024, 256, 0},  // 400K: 0.0184 against 0.0255 ms/iter (W = 512)
+    {448u * 1024, 1024, 0},  // 448K: 0.0181 against 0.0250 ms/iter (W = 512)
+    {576u * 1024, 1536, 0},  // 576K: 0.0212 against 0.0270 ms/iter (W = 512)
+    {640u * 1024, 256, 0},  // 640K: 0.0183 against 0.0308 ms/iter (W = 1024)
+    {672u * 1024, 1792, 0},  // 672K: 0.0232 against 0.0293 ms/iter (W = 512)
+    {768u * 1024, 256, 0},  // 768K: 0.0217 against 0.0248 ms/iter (W = 512)
+    {784u * 1024, 1792, 0},  // 784K: 0.0264 against 0.0298 ms/iter (W = 512)
+    {896u * 1024, 256, 0},  // 896K: 0.0223 against 0.0342 ms/iter (W = 1024)
+    {1024u * 1024, 512, 0},  // 1024K: 0.0203 against 0.0249 ms/iter (W = 1024)
+    {1280u * 1024, 256, 0},  // 1280K: 0.0285 against 0.0342 ms/iter (W = 1280)
+    {1296u * 1024, 2304, 0},  // 1296K: 0.0292 against 0.0410 ms/iter (W = 1024)
+    {1344u * 1024, 1024, 32},  // 1344K: 0.0322 against 0.0364 ms/iter (W = 1024)
+    {1440u * 1024, 2560, 0},  // 1440K: 0.0334 against 0.0424 ms/iter (W = 1024)
+    {1568u * 1024, 512, 0},  // 1568K: 0.0322 against 0.0373 ms/iter (W = 1024)
+    {1600u * 1024, 1024, 32},  // 1600K: 0.0373 against 0.0417 ms/iter (W = 1024)
+    {2160u * 1024, 512, 0},  // 2160K: 0.0474 against 0.0559 ms/iter (W = 1536)
+    {2880u * 1024, 2560, 0},  // 2880K: 0.0626 against 0.0794 ms/iter (W = 2048)
+    {3024u * 1024, 512, 0},  // 3024K: 0.0678 against 0.0768 ms/iter (W = 2304)
+    {3600u * 1024, 2304, 0},  // 3600K: 0.0879 against 0.0968 ms/iter (W = 1024)
+    {5120u * 1024, 1280, 0},  // 5120K: 0.0955 against 0.1032 ms/iter (W = 2048)
+    {7200u * 1024, 1280, 0},  // 7200K: 0.1653 against 0.1885 ms/iter (W = 2048)
+    {7776u * 1024, 1536, 0},  // 7776K: 0.1807 against 0.2043 ms/iter (W = 2048)
+    {9216u * 1024, 1536, 0},  // 9216K: 0.1826 against 0.1994 ms/iter (W = 2048)
+    {9408u * 1024, 3072, 0},  // 9408K: 0.2007 against 0.2243 ms/iter (W = 2048)
+    {10240u * 1024, 1280, 0},  // 10240K: 0.1980 against 0.2223 ms/iter (W = 2048)
+    {10800u * 1024, 2560, 0},  // 10800K: 0.2847 against 0.3449 ms/iter (W = 2304)
+    {12288u * 1024, 3072, 0},  // 12288K: 0.2316 against 0.2559 ms/iter (W = 2048)
+    {14336u * 1024, 1792, 0},  // 14336K: 0.2879 against 0.4295 ms/iter (W = 3584)
+    {16384u * 1024, 2048, 0},  // 16384K: 0.3229 against 0.4005 ms/iter (W = 4096)
+    {27216u * 1024, 4096, 0},  // 27216K: 0.8166 against 0.9911 ms/iter (W = 3584)
+    {28000u * 1024, 4096, 0},  // 28000K: 0.8687 against 1.0280 ms/iter (W = 3584)
+    {28672u * 1024, 4096, 0},  // 28672K: 0.7620 against 0.9017 ms/iter (W = 3584)
+    {0, 0, 0},
+};
+
+static bool tuning_is_default(const ll_tuning *t) {
+  return !t || (t->width == 0 && t->rows_per_cta == 0 && t->threads_wide == 0 && t->threads_tall == 0 &&
+                t->kernels == 0 && t->cluster_variant == 0);
+}
+
+// The tuning a context of length n runs with: the caller's, or the measured
+// preference for n when the caller leaves every choice to the engine.
+static const ll_tuning *effective_tuning(uint32_t n, const ll_tuning *t, ll_tuning &store) {
+  if (!tuning_is_default(t)) return t;
+  for (const auto &p : kPreferred)
+    if (p.n && p.n == n) {
+      store = t ? *t : ll_tuning{};
+      store.width = p.width;
+      store.kernels = p.kernels;
+      return &store;
+    }
+  return t;
+}
+
 struct ll_ctx {
   int device = 0;
   uint32_t q = 0, n = 0, b = 0, qn = 0;
@@ -1025,6 +1097,8 @@ ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
   if (!out) return LL_ERR_ARG;
   *out = nullptr;
   if (n < 64 || n % 4 || q <= n || q > 0x7fffffffu || (q & 1) == 0) return LL_ERR_ARG;
+  ll_tuning pref{};
+  tuning = effective_tuning(n, tuning, pref);
   Shape s;
   if (!choose_shape((long long)n / 2, tuning, s)) return LL_ERR_SHAPE;
   ll_ctx *ctx = new ll_ctx();
@@ -1475,6 +1549,8 @@ ll_status ll_device_restore(ll_ctx *ctx, uint32_t *offset) {
 }
 
 uint64_t ll_context_bytes(uint32_t q, uint32_t n, const ll_tuning *tuning) {
+  ll_tuning pref{};
+  tuning = effective_tuning(n, tuning, pref);
   Shape s;
   if (n < 64 || n % 4 || !choose_shape((long long)n / 2, tuning, s)) return 0;
   (void)q;
@@ -1548,6 +1624,14 @@ void ll_shape(const ll_ctx *ctx, int32_t *width, int32_t *height, int32_t *rows_
 const char *ll_last_error(const ll_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 int32_t ll_check_tables(void) {
   int32_t bad = 0;
+  for (const auto &p : kPreferred) {
+    if (!p.n) continue;
+    ll_tuning t{};
+    t.width = p.width;
+    t.kernels = p.kernels;
+    Shape s;
+    if (!choose_shape((long long)p.n / 2, &t, s) || s.W != p.width || !s.sw || !s.st) ++bad;
+  }
   for (const auto &k : kWide)
     if ((int)stage_twiddles(k.rad, k.nrad).size() != k.extra) ++bad;
   for (const auto &k : kTall)

@@ -80,6 +80,8 @@ typedef struct {
                                      (rows in shared memory, 8 elements per thread) */
 
 /* Creates a context for exponent q at FFT length n (FP64 words) on `device`.
+ * With tuning NULL (or all zero) the engine chooses the launch: for some
+ * lengths from a built-in table of shapes measured fastest on the B200.
  * Replaces alloc_gpu_mem + write_gpu_data (CUDALucas.cu:1096, :1125).
  * n must be even, n/2 must factor into a supported W x H split, q > n. */
 ll_status ll_create(int device, uint32_t q, uint32_t n, const ll_tuning *tuning,
@@ -151,8 +153,9 @@ const char *ll_last_error(const ll_ctx *ctx); /* text of the last failure   */
 int32_t ll_kernel_kinds(const ll_ctx *ctx);
 /* Host-only self-check of the compiled kernel tables: the number of
  * specialised kernels whose stage-twiddle table (built on the host from the
- * recorded radix list) does not have the size the kernel reads.  0 when
- * consistent; needs no GPU. */
+ * recorded radix list) does not have the size the kernel reads, plus the
+ * built-in launch preferences that do not give a specialised shape of their
+ * width.  0 when consistent; needs no GPU. */
 int32_t ll_check_tables(void);
 const char *ll_status_string(ll_status s);
 

@@ -371,3 +371,32 @@ def test_long_lengths_columns_agree_with_generic_kernels(nk):
     assert np.array_equal(cl.standardize(d1, q, n)[0], cl.standardize(d2, q, n)[0])
     assert cl.digits_res64(d1, q, n, o1) == cl.digits_res64(d2, q, n, o2)
     assert e1 < 0.4 and e2 < 0.4
+
+
+@pytest.mark.parametrize("nk", [288, 640, 1296, 1344, 1440, 2880, 14336])
+def test_preferred_shapes_agree_with_heuristic_shapes(nk):
+    """Lengths with a built-in launch preference (a row width, and for some
+    the alternative row kernel, measured faster than the width nearest
+    sqrt(N)) give the digits of the heuristic shape (any explicit tuning
+    skips the preference) and the oracle's residue."""
+    n = nk * 1024
+    q = _exponent_at(n)
+    off = q // 5
+    d1, o1, e1, s1 = engine_run(q, n, off, 40)
+    d2, o2, e2, s2 = engine_run(q, n, off, 40, kernels=cl.native.LL_KERNELS_NO_CLUSTER)
+    assert (s1["W"], s1["threads_wide"]) != (s2["W"], s2["threads_wide"]), (s1, s2)
+    assert s1["wide_specialised"] and s1["tall_specialised"]
+    assert o1 == o2
+    assert np.array_equal(cl.standardize(d1, q, n)[0], cl.standardize(d2, q, n)[0])
+    assert e1 < 0.4 and e2 < 0.4
+    if n <= 2 * 1024 * 1024:
+        from oracle.binding import set_threads
+        set_threads(16)
+        try:
+            o = Oracle(q, n)
+            o.start(off)
+            o.step(40)
+            want = o.res64()
+        finally:
+            set_threads(1)
+        assert cl.digits_res64(d1, q, n, o1) == want
