@@ -67,10 +67,10 @@ typedef struct {
  * (measured slower at 12K and 14K, equal at 56K, so not the default);
  * LL_KERNELS_NO_PREFETCH turns off the L2 prefetch that lengths larger than
  * L2 use.  Short lengths with a cluster-resident kernel (8K, 10K, 12K, 14K,
- * 16K, 18K, 20K, 32K, 36K, 42K, 48K, 56K) run each ll_step as one launch of one thread-block cluster whose
- * shared memory holds the whole state; LL_KERNELS_NO_CLUSTER turns that off
- * (two launches per iteration), LL_KERNELS_CLUSTER8 keeps to the portable
- * cluster size of 8 CTAs. */
+ * 16K, 18K, 20K, 32K, 36K, 42K, 48K, 56K) run each ll_step as one launch of
+ * one thread-block cluster whose shared memory holds the whole state;
+ * LL_KERNELS_NO_CLUSTER turns that off (two launches per iteration),
+ * LL_KERNELS_CLUSTER8 keeps to the portable cluster size of 8 CTAs. */
 #define LL_KERNELS_GENERIC 1
 #define LL_KERNELS_FUSED 2
 #define LL_KERNELS_NO_PREFETCH 4  /* no L2 prefetch of the next wave's data */
